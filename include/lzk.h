@@ -1,0 +1,162 @@
+/* lzk.h -- C ABI of the B200 Groth16 prover hot path (BN254).
+ *
+ * Drop-in boundary for the operator and protocol layer of LibLightZK
+ * (include/operator/msm.cuh, include/operator/poly.cuh,
+ * include/protocol/groth16.cuh).  The reference exposes these as C++
+ * templates called with device pointers on the default stream; this ABI
+ * exposes the same operators as plain extern "C" functions over device
+ * pointers, an explicit CUDA stream (passed as void*, may be NULL for the
+ * legacy default stream) and an int status.
+ *
+ * Data layout (bit-identical to the reference's host arithmetic, so host
+ * arrays of libff::alt_bn128_* values can be copied to the device as is):
+ *   lzk_fr_t / lzk_fq_t  four little-endian 64-bit limbs, Montgomery form
+ *                        with R = 2^256 (fp.cuh:33).
+ *   lzk_fq2_t            c0 + c1*i, i^2 = -1 (alt_bn128_init.cu:77).
+ *   lzk_g1_t, lzk_g2_t   Jacobian (X, Y, Z), the layouts of
+ *                        libff::alt_bn128_G1 / alt_bn128_G2
+ *                        (alt_bn128_g1.cuh:27, alt_bn128_g2.cuh:28).
+ *   lzk_g1_affine_t ...  affine (x, y); the point at infinity is x = y = 0.
+ *
+ * Every function returns LZK_OK (0) or a negative LZK_E* code and never
+ * aborts the process.  Work is enqueued on `stream` and completes
+ * asynchronously unless stated otherwise.
+ */
+#ifndef LZK_H
+#define LZK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LZK_OK            0
+#define LZK_EINVAL       -1   /* bad argument (size, alignment, null) */
+#define LZK_ENOMEM       -2   /* device allocation failed */
+#define LZK_ETIMEOUT     -3   /* a bounded device-side wait gave up */
+#define LZK_EDEVICE      -4   /* CUDA runtime error */
+#define LZK_EUNSUPPORTED -5   /* configuration not supported */
+#define LZK_EBUSY        -6   /* admission refused (memory budget) */
+
+typedef struct { uint64_t limb[4]; } lzk_fr_t;
+typedef struct { uint64_t limb[4]; } lzk_fq_t;
+typedef struct { lzk_fq_t c0, c1; } lzk_fq2_t;
+typedef struct { lzk_fq_t x, y; } lzk_g1_affine_t;
+typedef struct { lzk_fq2_t x, y; } lzk_g2_affine_t;
+typedef struct { lzk_fq_t X, Y, Z; } lzk_g1_t;
+typedef struct { lzk_fq2_t X, Y, Z; } lzk_g2_t;
+
+/* Human-readable text for a status code. */
+const char* lzk_status_string(int status);
+/* Library version string. */
+const char* lzk_version(void);
+
+/* ------------------------------------------------------------------ MSM
+ * out = sum_i scalars[i] * bases[i], a Pippenger bucket method with signed
+ * c-bit digits, counting-sorted bucket lists and XYZZ accumulation.
+ * Replaces multi_scalar_multiplication_g1/_g2 (msm.cuh:210-247).
+ *
+ * scalars : n Fr elements, Montgomery form (as the reference's MSM takes
+ *           them, msm.cuh:83-84).
+ * bases   : with flags = 0, n affine points.
+ *           With LZK_MSM_PRECOMPUTED, a table of `precomp_windows` shifted
+ *           copies: entry (j, i) at bases[j * level_stride + i] holds
+ *           2^(j * window_bits) * P_i in affine form -- the layout that
+ *           pre_comp_g1/_g2 build (msm.cuh:48-75, points[i + j*length]),
+ *           with affine entries.  Every window then shares one set of
+ *           buckets, so no doubling chain combines the windows.
+ * out     : one Jacobian point (device memory).
+ * cfg     : may be NULL (autotuned window width, library-managed scratch).
+ */
+#define LZK_MSM_PRECOMPUTED 0x1u
+
+typedef struct lzk_msm_cfg {
+    uint32_t window_bits;     /* c; 0 = autotune.  Must equal the table's
+                                 window width with LZK_MSM_PRECOMPUTED.     */
+    uint32_t flags;           /* LZK_MSM_* */
+    uint32_t precomp_windows; /* shifted copies in the table (PRECOMPUTED) */
+    uint32_t reserved;
+    size_t level_stride;      /* points between copies (PRECOMPUTED)        */
+    void* workspace;          /* optional device scratch; NULL = allocate
+                                 stream-ordered from the device pool        */
+    size_t workspace_bytes;
+} lzk_msm_cfg;
+
+int lzk_msm_g1(const lzk_fr_t* scalars, const lzk_g1_affine_t* bases, size_t n,
+               lzk_g1_t* out, const lzk_msm_cfg* cfg, void* stream);
+int lzk_msm_g2(const lzk_fr_t* scalars, const lzk_g2_affine_t* bases, size_t n,
+               lzk_g2_t* out, const lzk_msm_cfg* cfg, void* stream);
+/* Scratch bytes lzk_msm_g1/_g2 need for this n and cfg (group 1 or 2). */
+size_t lzk_msm_workspace_bytes(int group, size_t n, const lzk_msm_cfg* cfg);
+/* Window width the autotuner picks for an MSM of n points (group 1 or 2,
+ * precomputed or not). */
+uint32_t lzk_msm_autotune_window(int group, size_t n, uint32_t flags);
+
+/* Build the shifted-copy table for LZK_MSM_PRECOMPUTED: table[j*level_stride
+ * + i] = 2^(j*window_bits) * bases[i], affine, j < windows.  Replaces
+ * pre_comp_g1/_g2 (msm.cuh:48-75).  level_stride >= n. */
+int lzk_g1_precompute(const lzk_g1_affine_t* bases, size_t n, uint32_t window_bits,
+                      uint32_t windows, lzk_g1_affine_t* table, size_t level_stride, void* stream);
+int lzk_g2_precompute(const lzk_g2_affine_t* bases, size_t n, uint32_t window_bits,
+                      uint32_t windows, lzk_g2_affine_t* table, size_t level_stride, void* stream);
+/* Windows a table needs for window width c: ceil(255 / c). */
+uint32_t lzk_msm_precomp_windows(uint32_t window_bits);
+
+/* Jacobian <-> affine conversion on the device (batch inversion). */
+int lzk_g1_to_affine(const lzk_g1_t* in, lzk_g1_affine_t* out, size_t n, void* stream);
+int lzk_g2_to_affine(const lzk_g2_t* in, lzk_g2_affine_t* out, size_t n, void* stream);
+
+/* ------------------------------------------------------------------ NTT
+ * In-place transform of 2^log_n Fr elements (Montgomery form), natural order
+ * in and out.  Replaces number_theory_transformation (poly.cuh:65-73) with
+ * the roots of ntt-params.cuh: forward X_k = sum_j a_j w^(jk), w the
+ * 2^log_n-th root of the table; inverse uses w^-1 and scales by 2^-log_n;
+ * the coset forms evaluate on / interpolate from g*<w>, g = 5
+ * (alt_bn128_init.cu:50): COSET_FORWARD multiplies a_j by g^j first,
+ * COSET_INVERSE multiplies the result by g^-j.  log_n <= 26. */
+#define LZK_NTT_FORWARD       0
+#define LZK_NTT_INVERSE       1
+#define LZK_NTT_COSET_FORWARD 2
+#define LZK_NTT_COSET_INVERSE 3
+
+int lzk_ntt(lzk_fr_t* data, uint32_t log_n, int direction, void* stream);
+/* `count` transforms of the same size, transform t at data + t*stride. */
+int lzk_ntt_batch(lzk_fr_t* data, uint32_t log_n, uint32_t count, size_t stride, int direction, void* stream);
+/* Build this device's twiddle tables for size 2^log_n now (they are
+ * otherwise built on first use, synchronously; call before stream capture). */
+int lzk_ntt_prepare(uint32_t log_n);
+/* The reference's own signature (poly.cuh:65-66): omega_powers is the
+ * caller's table (omega_powers[e] = w^e, e < deg/2, as ntt_setup builds it,
+ * groth16-operator.cuh:6-31) and factor an optional device scalar applied
+ * to every output. */
+int lzk_number_theory_transformation(size_t deg, size_t log_deg, lzk_fr_t* coeffs, const lzk_fr_t* omega_powers,
+                                     const lzk_fr_t* factor, void* stream);
+
+/* ------------------------------------------------------------------ SpMV
+ * R1CS evaluation out = M*z over Fr (Montgomery).  Replaces
+ * batch_sparse_matrix_vector_multiplication (poly.cuh:5-30) and its
+ * descriptor xpu::spmat_descript (xpu-spmat.cuh:20-25).  Row i covers
+ * [row_ptr[i], row_ptr[i+1]); the last row ends at nnz, so both the
+ * reference's `rows`-entry row_ptr and a standard rows+1 one work.
+ * index_bytes = 8 for the reference's size_t arrays, 4 for uint32. */
+typedef struct lzk_csr {
+    const lzk_fr_t* val;
+    const void* col_idx;
+    const void* row_ptr;
+    uint64_t rows, cols, nnz;
+    uint32_t index_bytes;
+    uint32_t reserved;
+} lzk_csr;
+
+/* Az, Bz, Cz in one launch; a NULL matrix skips its output. */
+int lzk_spmv3(const lzk_csr* A, const lzk_csr* B, const lzk_csr* C, const lzk_fr_t* z,
+              lzk_fr_t* Az, lzk_fr_t* Bz, lzk_fr_t* Cz, void* stream);
+int lzk_spmv(const lzk_csr* M, const lzk_fr_t* z, lzk_fr_t* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LZK_H */

@@ -1,0 +1,170 @@
+// curve.cuh -- Fq2 and BN254 curve arithmetic for G1 (over Fq) and G2 (over
+// Fq2), generic in the coordinate field.
+//
+// Three point forms:
+//   Aff<F>  {x, y}          bases in HBM (64 B for G1, 128 B for G2); the
+//                           point at infinity is x = y = 0 (not on the curve).
+//   XYZZ<F> {X, Y, ZZ, ZZZ} bucket accumulators: x = X/ZZ, y = Y/ZZZ; the
+//                           point at infinity is ZZ = 0.  Mixed addition costs
+//                           8M+2S and needs no inversion.
+//   Jac<F>  {X, Y, Z}       the reference's output form, x = X/Z^2,
+//                           y = Y/Z^3 (alt_bn128_g1.cuh:27); the point at
+//                           infinity is written as (0, 1, 0) like libff's
+//                           G1_zero (alt_bn128_init.cu:127-129).
+// The XYZZ formulas are the published "xyzz" set for short Weierstrass
+// curves with a = 0 (Bernstein-Lange EFD: madd-2008-s, mdbl-2008-s-1,
+// add-2008-s, dbl-2008-s-1); results are compared with the reference only
+// after normalisation to affine, which is representation independent.
+#pragma once
+#include "field.cuh"
+
+namespace lzk {
+
+// ---------------- Fq2 = Fq[i] / (i^2 + 1) ----------------
+struct Fq2 {
+    Fq c0, c1;
+    __device__ __forceinline__ static Fq2 zero() { return {Fq::zero(), Fq::zero()}; }
+    __device__ __forceinline__ static Fq2 one() { return {Fq::one(), Fq::zero()}; }
+    __device__ __forceinline__ bool is_zero() const { return c0.is_zero() && c1.is_zero(); }
+    __device__ __forceinline__ bool operator==(const Fq2& o) const { return c0 == o.c0 && c1 == o.c1; }
+};
+__device__ __forceinline__ Fq2 add(const Fq2& a, const Fq2& b) { return {add(a.c0, b.c0), add(a.c1, b.c1)}; }
+__device__ __forceinline__ Fq2 sub(const Fq2& a, const Fq2& b) { return {sub(a.c0, b.c0), sub(a.c1, b.c1)}; }
+__device__ __forceinline__ Fq2 neg(const Fq2& a) { return {neg(a.c0), neg(a.c1)}; }
+__device__ __forceinline__ Fq2 dbl(const Fq2& a) { return {dbl(a.c0), dbl(a.c1)}; }
+// Karatsuba: 3 Fq products
+__device__ __forceinline__ Fq2 mul(const Fq2& a, const Fq2& b)
+{
+    Fq aa = mul(a.c0, b.c0), bb = mul(a.c1, b.c1);
+    Fq s = mul(add(a.c0, a.c1), add(b.c0, b.c1));
+    return {sub(aa, bb), sub(sub(s, aa), bb)};
+}
+// (a0 + a1 i)^2 = (a0+a1)(a0-a1) + 2 a0 a1 i: 2 Fq products
+__device__ __forceinline__ Fq2 sqr(const Fq2& a)
+{
+    Fq ab = mul(a.c0, a.c1);
+    return {mul(add(a.c0, a.c1), sub(a.c0, a.c1)), dbl(ab)};
+}
+static __device__ __noinline__ Fq2 inverse(const Fq2& a)
+{
+    Fq t = inverse(add(sqr(a.c0), sqr(a.c1)));
+    return {mul(a.c0, t), neg(mul(a.c1, t))};
+}
+
+// ---------------- point forms ----------------
+template <class F> struct Aff { F x, y; };
+template <class F> struct XYZZ { F X, Y, ZZ, ZZZ; };
+template <class F> struct Jac { F X, Y, Z; };
+
+template <class F> __device__ __forceinline__ bool aff_is_inf(const Aff<F>& p) { return p.x.is_zero() && p.y.is_zero(); }
+
+template <class F> __device__ __forceinline__ XYZZ<F> xyzz_inf() { return {F::zero(), F::zero(), F::zero(), F::zero()}; }
+template <class F> __device__ __forceinline__ bool xyzz_is_inf(const XYZZ<F>& p) { return p.ZZ.is_zero(); }
+template <class F> __device__ __forceinline__ XYZZ<F> xyzz_from_aff(const Aff<F>& a)
+{
+    if (aff_is_inf(a)) return xyzz_inf<F>();
+    return {a.x, a.y, F::one(), F::one()};
+}
+
+// 2*(x, y) for affine input (mdbl-2008-s-1)
+template <class F> __device__ __forceinline__ XYZZ<F> xyzz_mdbl(const Aff<F>& a)
+{
+    F U = dbl(a.y);
+    F V = sqr(U);
+    F W = mul(U, V);
+    F S = mul(a.x, V);
+    F x2 = sqr(a.x);
+    F M = add(dbl(x2), x2);
+    F X3 = sub(sqr(M), dbl(S));
+    F Y3 = sub(mul(M, sub(S, X3)), mul(W, a.y));
+    return {X3, Y3, V, W};
+}
+
+// 2*P (dbl-2008-s-1)
+template <class F> __device__ __forceinline__ XYZZ<F> xyzz_dbl(const XYZZ<F>& p)
+{
+    if (xyzz_is_inf(p)) return p;
+    F U = dbl(p.Y);
+    F V = sqr(U);
+    F W = mul(U, V);
+    F S = mul(p.X, V);
+    F x2 = sqr(p.X);
+    F M = add(dbl(x2), x2);
+    F X3 = sub(sqr(M), dbl(S));
+    F Y3 = sub(mul(M, sub(S, X3)), mul(W, p.Y));
+    return {X3, Y3, mul(V, p.ZZ), mul(W, p.ZZZ)};
+}
+
+// P + Q with Q affine (madd-2008-s); handles infinity, P == Q and P == -Q
+template <class F> __device__ __forceinline__ XYZZ<F> xyzz_madd(const XYZZ<F>& p, const Aff<F>& q)
+{
+    if (aff_is_inf(q)) return p;
+    if (xyzz_is_inf(p)) return xyzz_from_aff(q);
+    F U2 = mul(q.x, p.ZZ);
+    F S2 = mul(q.y, p.ZZZ);
+    F P = sub(U2, p.X);
+    F R = sub(S2, p.Y);
+    if (P.is_zero()) {
+        if (R.is_zero()) return xyzz_mdbl(q);
+        return xyzz_inf<F>();
+    }
+    F PP = sqr(P);
+    F PPP = mul(P, PP);
+    F Q = mul(p.X, PP);
+    F X3 = sub(sub(sqr(R), PPP), dbl(Q));
+    F Y3 = sub(mul(R, sub(Q, X3)), mul(p.Y, PPP));
+    return {X3, Y3, mul(p.ZZ, PP), mul(p.ZZZ, PPP)};
+}
+
+// P + Q (add-2008-s)
+template <class F> __device__ __forceinline__ XYZZ<F> xyzz_add(const XYZZ<F>& p, const XYZZ<F>& q)
+{
+    if (xyzz_is_inf(q)) return p;
+    if (xyzz_is_inf(p)) return q;
+    F U1 = mul(p.X, q.ZZ);
+    F U2 = mul(q.X, p.ZZ);
+    F S1 = mul(p.Y, q.ZZZ);
+    F S2 = mul(q.Y, p.ZZZ);
+    F P = sub(U2, U1);
+    F R = sub(S2, S1);
+    if (P.is_zero()) {
+        if (R.is_zero()) return xyzz_dbl(p);
+        return xyzz_inf<F>();
+    }
+    F PP = sqr(P);
+    F PPP = mul(P, PP);
+    F Q = mul(U1, PP);
+    F X3 = sub(sub(sqr(R), PPP), dbl(Q));
+    F Y3 = sub(mul(R, sub(Q, X3)), mul(S1, PPP));
+    return {X3, Y3, mul(mul(p.ZZ, q.ZZ), PP), mul(mul(p.ZZZ, q.ZZZ), PPP)};
+}
+
+template <class F> __device__ __forceinline__ XYZZ<F> xyzz_neg(const XYZZ<F>& p) { return {p.X, neg(p.Y), p.ZZ, p.ZZZ}; }
+
+// XYZZ -> Jacobian without inversion: Z = ZZ*ZZZ, X = X*ZZ*ZZZ^2, Y = Y*ZZ^3*ZZZ^2
+template <class F> __device__ __forceinline__ Jac<F> xyzz_to_jac(const XYZZ<F>& p)
+{
+    if (xyzz_is_inf(p)) return {F::zero(), F::one(), F::zero()};
+    F zzz2 = sqr(p.ZZZ);
+    F Z = mul(p.ZZ, p.ZZZ);
+    F X = mul(mul(p.X, p.ZZ), zzz2);
+    F zz3 = mul(sqr(p.ZZ), p.ZZ);
+    F Y = mul(mul(p.Y, zz3), zzz2);
+    return {X, Y, Z};
+}
+
+template <class F> __device__ __forceinline__ XYZZ<F> jac_to_xyzz(const Jac<F>& p)
+{
+    if (p.Z.is_zero()) return xyzz_inf<F>();
+    F z2 = sqr(p.Z);
+    return {p.X, p.Y, z2, mul(z2, p.Z)};
+}
+
+// Out-of-line copies for the cold kernels (fix-up, reduction levels, window
+// combination, table building): one body per kernel instead of one per call
+// site keeps code size and compile time down where the adds are not the
+// bottleneck.
+template <class F> __device__ __noinline__ XYZZ<F> xyzz_add_cold(const XYZZ<F> p, const XYZZ<F> q) { return xyzz_add(p, q); }
+template <class F> __device__ __noinline__ XYZZ<F> xyzz_dbl_cold(const XYZZ<F> p) { return xyzz_dbl(p); }
+
+}  // namespace lzk

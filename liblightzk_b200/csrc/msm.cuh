@@ -1,0 +1,313 @@
+// msm.cuh -- shared pieces of the Pippenger MSM (msm_sort.cu, msm_g1.cu,
+// msm_g2.cu).  See msm_sort.cu for the pipeline.
+#pragma once
+#include "common.cuh"
+#include "curve.cuh"
+
+namespace lzk {
+
+struct G1 { using F = Fq; };
+struct G2 { using F = Fq2; };
+
+constexpr uint32_t kAccChunk = 32;   // sorted entries per accumulation thread
+constexpr uint32_t kLevelL = 8;      // buckets per thread in a reduction level
+
+struct MsmPlan {
+    size_t n = 0;
+    uint32_t c = 0;        // window bits
+    uint32_t W = 0;        // digit windows
+    uint32_t nb = 0;       // buckets per window = 2^(c-1)
+    uint32_t wb = 0;       // bucket sets: W (plain) or 1 (shared, precomputed)
+    uint32_t B = 0;        // total buckets = wb * nb
+    bool shared = false;   // precomputed table: one bucket set for all windows
+    size_t stride = 0;     // table level stride
+    size_t max_entries = 0;
+    size_t chunks = 0;
+    // workspace offsets
+    size_t o_cnt, o_off, o_ent, o_bsum, o_head, o_tail, o_lr0, o_la0, o_lr1, o_la1, bytes;
+};
+
+inline uint32_t windows_for(uint32_t c) { return (255 + c - 1) / c; }
+
+template <class Gp>
+inline void plan_msm(MsmPlan& p, size_t n, uint32_t c, bool shared, size_t stride)
+{
+    using X = XYZZ<typename Gp::F>;
+    p.n = n; p.c = c; p.W = windows_for(c); p.nb = 1u << (c - 1);
+    p.shared = shared; p.stride = stride;
+    p.wb = shared ? 1 : p.W;
+    p.B = p.wb * p.nb;
+    p.max_entries = n * (size_t)p.W;
+    p.chunks = (p.max_entries + kAccChunk - 1) / kAccChunk;
+    size_t lvl = (p.B + kLevelL - 1) / kLevelL;
+    Carver cv;
+    p.o_cnt = cv.take<uint32_t>(p.B);
+    p.o_off = cv.take<uint32_t>(p.B + 1);
+    p.o_ent = cv.take<uint32_t>(p.max_entries ? p.max_entries : 1);
+    p.o_bsum = cv.take<X>(p.B);
+    p.o_head = cv.take<X>(p.chunks ? p.chunks : 1);
+    p.o_tail = cv.take<X>(p.chunks ? p.chunks : 1);
+    p.o_lr0 = cv.take<X>(lvl);
+    p.o_la0 = cv.take<X>(lvl);
+    p.o_lr1 = cv.take<X>(lvl);
+    p.o_la1 = cv.take<X>(lvl);
+    p.bytes = cv.off;
+}
+
+// counting sort of the signed digits of all scalars into bucket lists:
+// cnt/off/ent as carved by plan_msm (msm_sort.cu)
+int msm_sort(const MsmPlan& p, const Fr* scalars, uint32_t* cnt, uint32_t* off, uint32_t* ent, cudaStream_t st);
+uint32_t msm_autotune(int group, size_t n, bool shared);
+
+// largest b in [lo, B) with off[b] <= e
+__device__ __forceinline__ uint32_t bucket_of(const uint32_t* off, uint32_t lo, uint32_t B, uint32_t e)
+{
+    uint32_t hi = B;  // invariant: off[lo] <= e, answer in [lo, hi)
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (off[mid] <= e) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+template <class F>
+__device__ __forceinline__ Aff<F> load_base(const Aff<F>* bases, uint32_t v)
+{
+    Aff<F> p = ldg_elem(bases + (v & 0x7fffffffu));
+    if (v & 0x80000000u) { if (!aff_is_inf(p)) p.y = neg(p.y); }
+    return p;
+}
+
+template <class F>
+__global__ void __launch_bounds__(256) k_accumulate(const Aff<F>* __restrict__ bases, const uint32_t* __restrict__ ent,
+                                                    const uint32_t* __restrict__ off, uint32_t B, size_t chunks,
+                                                    XYZZ<F>* __restrict__ bsum, XYZZ<F>* __restrict__ head,
+                                                    XYZZ<F>* __restrict__ tail)
+{
+    uint64_t t = gtid();
+    if (t >= chunks) return;
+    uint32_t T = off[B];
+    uint64_t cs64 = t * kAccChunk;
+    if (cs64 >= T) return;
+    uint32_t cs = (uint32_t)cs64, ce = min(cs + kAccChunk, T);
+    uint32_t b = bucket_of(off, 0, B, cs);
+    uint32_t bbeg = off[b], bend = off[b + 1];
+    XYZZ<F> acc = xyzz_inf<F>();
+    for (uint32_t e = cs; e < ce; e++) {
+        if (e == bend) {
+            // bucket b finished inside this chunk
+            if (bbeg < cs) st_elem(head + t, acc); else st_elem(bsum + b, acc);
+            b = bucket_of(off, b + 1, B, e);
+            bbeg = off[b]; bend = off[b + 1];
+            acc = xyzz_inf<F>();
+        }
+        acc = xyzz_madd(acc, load_base(bases, ent[e]));
+    }
+    bool began_before = bbeg < cs, cont_after = bend > ce;
+    if (began_before) st_elem(head + t, acc);
+    else if (cont_after) st_elem(tail + t, acc);
+    else st_elem(bsum + b, acc);
+}
+
+template <class F>
+__global__ void k_fixup(const uint32_t* __restrict__ off, uint32_t B, XYZZ<F>* __restrict__ bsum,
+                        const XYZZ<F>* __restrict__ head, const XYZZ<F>* __restrict__ tail)
+{
+    for (uint64_t b = gtid(); b < B; b += gstride()) {
+        uint32_t s = off[b], e = off[b + 1];
+        if (s == e) continue;
+        uint32_t c0 = s / kAccChunk, c1 = (e - 1) / kAccChunk;
+        if (c0 == c1) continue;
+        XYZZ<F> acc = ld_elem(tail + c0);
+        for (uint32_t c = c0 + 1; c <= c1; c++) acc = xyzz_add_cold(acc, ld_elem(head + c));
+        st_elem(bsum + b, acc);
+    }
+}
+
+// One level of the weighted bucket sum.  Per window, the input holds m
+// points X_k; thread (w, s) covers X_{sL..sL+L-1} and writes
+//   R_s = sum_j X_{sL+j}
+//   A_s = sum_j Ain_{sL+j} + 2^logM * sum_j (j + base) X_{sL+j}
+// so that sum_k (k + base) X_k = sum_s t_s + L * sum_s s R_s at every level.
+template <class F>
+__global__ void k_level(const XYZZ<F>* __restrict__ inR, const XYZZ<F>* __restrict__ inA,
+                        const uint32_t* __restrict__ off, uint32_t windows, uint32_t m, uint32_t L,
+                        uint32_t base, uint32_t logM, XYZZ<F>* __restrict__ outR, XYZZ<F>* __restrict__ outA)
+{
+    uint32_t segs = m / L;
+    uint64_t total = (uint64_t)windows * segs;
+    for (uint64_t t = gtid(); t < total; t += gstride()) {
+        uint32_t w = (uint32_t)(t / segs), s = (uint32_t)(t % segs);
+        size_t first = (size_t)w * m + (size_t)s * L;
+        XYZZ<F> run = xyzz_inf<F>(), acc = xyzz_inf<F>(), A = xyzz_inf<F>();
+        for (int j = (int)L - 1; j >= 0; j--) {
+            size_t k = first + j;
+            XYZZ<F> x = (off && off[k] == off[k + 1]) ? xyzz_inf<F>() : ld_elem(inR + k);
+            run = xyzz_add_cold(run, x);
+            if (j > 0 || base) acc = xyzz_add_cold(acc, run);
+            if (inA) A = xyzz_add_cold(A, ld_elem(inA + k));
+        }
+        for (uint32_t d = 0; d < logM; d++) acc = xyzz_dbl_cold(acc);
+        st_elem(outR + t, run);
+        st_elem(outA + t, xyzz_add_cold(A, acc));
+    }
+}
+
+template <class F>
+__global__ void k_finish(const XYZZ<F>* __restrict__ win, uint32_t windows, uint32_t c, Jac<F>* out)
+{
+    if (gtid() != 0) return;
+    XYZZ<F> r = xyzz_inf<F>();
+    for (int w = (int)windows - 1; w >= 0; w--) {
+        if (w != (int)windows - 1)
+            for (uint32_t d = 0; d < c; d++) r = xyzz_dbl_cold(r);
+        r = xyzz_add_cold(r, ld_elem(win + w));
+    }
+    st_elem(out, xyzz_to_jac(r));
+}
+
+template <class F>
+__global__ void k_write_inf(Jac<F>* out)
+{
+    if (gtid() == 0) st_elem(out, Jac<F>{F::zero(), F::one(), F::zero()});
+}
+
+template <class Gp>
+int run_msm(const Fr* scalars, const Aff<typename Gp::F>* bases, size_t n, Jac<typename Gp::F>* out,
+                   const lzk_msm_cfg* cfg, cudaStream_t st, uint32_t c_auto)
+{
+    using F = typename Gp::F;
+    using X = XYZZ<F>;
+    if (!out || (n && (!scalars || !bases))) return LZK_EINVAL;
+    if (n >= (1ull << 31)) return LZK_EINVAL;
+    uint32_t flags = cfg ? cfg->flags : 0u;
+    bool shared = (flags & LZK_MSM_PRECOMPUTED) != 0;
+    uint32_t c = (cfg && cfg->window_bits) ? cfg->window_bits : c_auto;
+    if (c < 2 || c > 24) return LZK_EINVAL;
+    size_t stride = shared ? cfg->level_stride : 0;
+    if (shared) {
+        if (!cfg->window_bits) return LZK_EINVAL;
+        if (cfg->precomp_windows < windows_for(c) || stride < n) return LZK_EINVAL;
+        if ((size_t)windows_for(c) * stride >= (1ull << 31)) return LZK_EINVAL;
+    }
+    if (n == 0) {
+        k_write_inf<F><<<1, 32, 0, st>>>(out);
+        return launch_status();
+    }
+    MsmPlan p;
+    plan_msm<Gp>(p, n, c, shared, stride);
+    Scratch ws;
+    LZK_TRY(ws.acquire(p.bytes, cfg ? cfg->workspace : nullptr, cfg ? cfg->workspace_bytes : 0, st));
+    char* base = ws.base;
+    uint32_t* cnt = reinterpret_cast<uint32_t*>(base + p.o_cnt);
+    uint32_t* off = reinterpret_cast<uint32_t*>(base + p.o_off);
+    uint32_t* ent = reinterpret_cast<uint32_t*>(base + p.o_ent);
+    X* bsum = reinterpret_cast<X*>(base + p.o_bsum);
+    X* head = reinterpret_cast<X*>(base + p.o_head);
+    X* tail = reinterpret_cast<X*>(base + p.o_tail);
+    X* lr[2] = {reinterpret_cast<X*>(base + p.o_lr0), reinterpret_cast<X*>(base + p.o_lr1)};
+    X* la[2] = {reinterpret_cast<X*>(base + p.o_la0), reinterpret_cast<X*>(base + p.o_la1)};
+
+    LZK_TRY(msm_sort(p, scalars, cnt, off, ent, st));
+    k_accumulate<F><<<grid_for(p.chunks, 256), 256, 0, st>>>(bases, ent, off, p.B, p.chunks, bsum, head, tail);
+    k_fixup<F><<<grid_for(p.B, 256, 148 * 8), 256, 0, st>>>(off, p.B, bsum, head, tail);
+    LZK_TRY(launch_status());
+
+    // weighted sums per bucket set
+    const X* inR = bsum; const X* inA = nullptr; const uint32_t* offp = off;
+    uint32_t m = p.nb, logM = 0, base1 = 1, pp = 0;
+    X* resA = nullptr;
+    while (true) {
+        uint32_t L = m < kLevelL ? m : kLevelL;
+        uint32_t segs = m / L;
+        size_t threads = (size_t)p.wb * segs;
+        k_level<F><<<grid_for(threads, 128), 128, 0, st>>>(inR, inA, offp, p.wb, m, L, base1, logM, lr[pp], la[pp]);
+        inR = lr[pp]; inA = la[pp]; resA = la[pp];
+        offp = nullptr; base1 = 0;
+        uint32_t lg = 0; while ((1u << lg) < L) lg++;
+        logM += lg;
+        m = segs;
+        pp ^= 1;
+        if (m == 1) break;
+    }
+    k_finish<F><<<1, 32, 0, st>>>(resA, p.wb, c, out);
+    return launch_status();
+}
+
+// ------------------------- precomputed shifted bases -------------------------
+template <class F>
+__global__ void k_precompute(const Aff<F>* __restrict__ bases, size_t n, uint32_t c, uint32_t windows,
+                             Aff<F>* __restrict__ table, size_t stride)
+{
+    // windows are normalised in groups of G with one inversion per group
+    constexpr int G = 8;
+    for (uint64_t i = gtid(); i < n; i += gstride()) {
+        Aff<F> P = ldg_elem(bases + i);
+        st_elem(table + i, P);
+        if (aff_is_inf(P)) {
+            Aff<F> z{F::zero(), F::zero()};
+            for (uint32_t j = 1; j < windows; j++) st_elem(table + (size_t)j * stride + i, z);
+            continue;
+        }
+        XYZZ<F> cur = xyzz_from_aff(P);
+        for (uint32_t j0 = 1; j0 < windows; j0 += G) {
+            int cntg = (int)min((uint32_t)G, windows - j0);
+            XYZZ<F> pts[G];
+            F pre[G];
+            F acc = F::one();
+            for (int k = 0; k < cntg; k++) {
+                for (uint32_t d = 0; d < c; d++) cur = xyzz_dbl_cold(cur);
+                pts[k] = cur;
+                acc = mul(acc, mul(cur.ZZ, cur.ZZZ));
+                pre[k] = acc;
+            }
+            F inv = inverse(acc);
+            for (int k = cntg - 1; k >= 0; k--) {
+                F dinv = k ? mul(inv, pre[k - 1]) : inv;  // (ZZ_k ZZZ_k)^-1
+                inv = mul(inv, mul(pts[k].ZZ, pts[k].ZZZ));
+                // x = X / ZZ = X * ZZZ * dinv,  y = Y / ZZZ = Y * ZZ * dinv
+                Aff<F> a{mul(mul(pts[k].X, dinv), pts[k].ZZZ), mul(mul(pts[k].Y, dinv), pts[k].ZZ)};
+                st_elem(table + (size_t)(j0 + k) * stride + i, a);
+            }
+        }
+    }
+}
+
+// Jacobian -> affine, 8 points per thread with one inversion
+template <class F>
+__global__ void k_jac_to_aff(const Jac<F>* __restrict__ in, Aff<F>* __restrict__ out, size_t n)
+{
+    constexpr int G = 8;
+    for (uint64_t t = gtid(); t * G < n; t += gstride()) {
+        size_t b = t * G;
+        int cntp = (int)((n - b) < G ? (n - b) : G);
+        F pre[G];
+        F acc = F::one();
+        for (int k = 0; k < cntp; k++) {
+            Jac<F> J = ld_elem(in + b + k);
+            if (!J.Z.is_zero()) acc = mul(acc, J.Z);
+            pre[k] = acc;
+        }
+        F inv = inverse(acc);
+        for (int k = cntp - 1; k >= 0; k--) {
+            Jac<F> J = ld_elem(in + b + k);
+            if (J.Z.is_zero()) { st_elem(out + b + k, Aff<F>{F::zero(), F::zero()}); continue; }
+            F zi = k ? mul(inv, pre[k - 1]) : inv;
+            inv = mul(inv, J.Z);
+            F z2 = sqr(zi);
+            st_elem(out + b + k, Aff<F>{mul(J.X, z2), mul(J.Y, mul(z2, zi))});
+        }
+    }
+}
+
+template <class F>
+int run_precompute(const Aff<F>* bases, size_t n, uint32_t c, uint32_t windows, Aff<F>* table,
+                          size_t stride, cudaStream_t st)
+{
+    if (!bases || !table || c < 2 || c > 24 || windows == 0 || windows > 256 || stride < n) return LZK_EINVAL;
+    if (n == 0) return LZK_OK;
+    k_precompute<F><<<grid_for(n, 64), 64, 0, st>>>(bases, n, c, windows, table, stride);
+    return launch_status();
+}
+
+}  // namespace lzk

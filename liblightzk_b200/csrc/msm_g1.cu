@@ -1,0 +1,33 @@
+// msm_g1.cu -- G1 instantiation of the MSM, the shifted-base table
+// builder and the Jacobian -> affine converter (templates in msm.cuh).
+#include "msm.cuh"
+
+using namespace lzk;
+
+extern "C" {
+
+int lzk_msm_g1(const lzk_fr_t* scalars, const lzk_g1_affine_t* bases, size_t n, lzk_g1_t* out,
+               const lzk_msm_cfg* cfg, void* stream)
+{
+    bool shared = cfg && (cfg->flags & LZK_MSM_PRECOMPUTED);
+    return run_msm<G1>(reinterpret_cast<const Fr*>(scalars), reinterpret_cast<const Aff<Fq>*>(bases), n,
+                       reinterpret_cast<Jac<Fq>*>(out), cfg, as_stream(stream), msm_autotune(1, n, shared));
+}
+
+int lzk_g1_precompute(const lzk_g1_affine_t* bases, size_t n, uint32_t window_bits, uint32_t windows,
+                      lzk_g1_affine_t* table, size_t level_stride, void* stream)
+{
+    return run_precompute<Fq>(reinterpret_cast<const Aff<Fq>*>(bases), n, window_bits, windows,
+                              reinterpret_cast<Aff<Fq>*>(table), level_stride, as_stream(stream));
+}
+
+int lzk_g1_to_affine(const lzk_g1_t* in, lzk_g1_affine_t* out, size_t n, void* stream)
+{
+    if ((!in || !out) && n) return LZK_EINVAL;
+    if (!n) return LZK_OK;
+    k_jac_to_aff<Fq><<<grid_for((n + 7) / 8, 128), 128, 0, as_stream(stream)>>>(
+        reinterpret_cast<const Jac<Fq>*>(in), reinterpret_cast<Aff<Fq>*>(out), n);
+    return launch_status();
+}
+
+}  // extern "C"

@@ -1,0 +1,33 @@
+// msm_g2.cu -- G2 instantiation of the MSM, the shifted-base table
+// builder and the Jacobian -> affine converter (templates in msm.cuh).
+#include "msm.cuh"
+
+using namespace lzk;
+
+extern "C" {
+
+int lzk_msm_g2(const lzk_fr_t* scalars, const lzk_g2_affine_t* bases, size_t n, lzk_g2_t* out,
+               const lzk_msm_cfg* cfg, void* stream)
+{
+    bool shared = cfg && (cfg->flags & LZK_MSM_PRECOMPUTED);
+    return run_msm<G2>(reinterpret_cast<const Fr*>(scalars), reinterpret_cast<const Aff<Fq2>*>(bases), n,
+                       reinterpret_cast<Jac<Fq2>*>(out), cfg, as_stream(stream), msm_autotune(2, n, shared));
+}
+
+int lzk_g2_precompute(const lzk_g2_affine_t* bases, size_t n, uint32_t window_bits, uint32_t windows,
+                      lzk_g2_affine_t* table, size_t level_stride, void* stream)
+{
+    return run_precompute<Fq2>(reinterpret_cast<const Aff<Fq2>*>(bases), n, window_bits, windows,
+                               reinterpret_cast<Aff<Fq2>*>(table), level_stride, as_stream(stream));
+}
+
+int lzk_g2_to_affine(const lzk_g2_t* in, lzk_g2_affine_t* out, size_t n, void* stream)
+{
+    if ((!in || !out) && n) return LZK_EINVAL;
+    if (!n) return LZK_OK;
+    k_jac_to_aff<Fq2><<<grid_for((n + 7) / 8, 128), 128, 0, as_stream(stream)>>>(
+        reinterpret_cast<const Jac<Fq2>*>(in), reinterpret_cast<Aff<Fq2>*>(out), n);
+    return launch_status();
+}
+
+}  // extern "C"

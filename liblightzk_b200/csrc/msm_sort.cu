@@ -1,0 +1,169 @@
+// msm_sort.cu -- Pippenger multi-scalar multiplication for BN254 G1 and G2.
+//
+// Replaces multi_scalar_multiplication_g1/_g2 of the reference
+// (include/operator/msm.cuh:210-247) and its kernels (msm.cuh:77-208).
+// Pipeline per call, all on one stream, no host synchronisation:
+//   1. k_count     signed c-bit digits of every scalar; a histogram of
+//                  (window, |digit|) buckets (global atomics).
+//   2. k_scan      exclusive prefix sum -> bucket offsets; off[B] = entries.
+//   3. k_scatter   counting-sort scatter of (point index, sign) entries.
+//   4. k_accumulate each thread adds exactly K consecutive sorted entries
+//                  (XYZZ mixed adds of affine bases), so the work is even
+//                  whatever the bucket sizes; segments that cross a chunk
+//                  boundary leave partial sums.
+//   5. k_fixup     folds those partial sums into their buckets.
+//   6. k_level     weighted bucket sums  sum_j j*B_j  by segmented running
+//                  sums, L buckets per thread, repeated until one value
+//                  per window is left.
+//   7. k_finish    windows combined by Horner (c doublings per window), or
+//                  nothing to combine when the bases come with precomputed
+//                  2^(c*w) shifts (every window shares one bucket set, the
+//                  scheme of msm.cuh:98-115 with pre_comp_g1's table).
+#include "msm.cuh"
+
+namespace lzk {
+
+// bits [lo, lo+c) of a canonical 254-bit scalar held as 8 limbs
+__device__ __forceinline__ uint32_t window_bits(const uint32_t s[8], uint32_t lo, uint32_t c)
+{
+    uint32_t w = lo >> 5, sh = lo & 31;
+    uint64_t v = s[w < 8 ? w : 7] >> sh;
+    if (w < 8 && sh) {
+        uint32_t hi = (w + 1 < 8) ? s[w + 1] : 0u;
+        v = ((uint64_t)s[w] | ((uint64_t)hi << 32)) >> sh;
+    } else if (w >= 8) {
+        v = 0;
+    }
+    return (uint32_t)v & ((1u << c) - 1u);
+}
+
+// Signed-digit recoding: raw = bits + carry in [0, 2^c]; raw > 2^(c-1) is
+// used as raw - 2^c with a carry into the next window.  |digit| <= 2^(c-1).
+struct DigitIter {
+    uint32_t s[8];
+    uint32_t carry = 0;
+    __device__ __forceinline__ void load(const Fr* sc)
+    {
+        Fr m = ldg_elem(sc);
+        Fr k = from_mont(m);
+        _Pragma("unroll") for (int i = 0; i < 8; i++) s[i] = k.v[i];
+        carry = 0;
+    }
+    // returns |digit| (0 = skip) and sets neg
+    __device__ __forceinline__ uint32_t next(uint32_t w, uint32_t c, bool& neg)
+    {
+        uint32_t raw = window_bits(s, w * c, c) + carry;
+        uint32_t half = 1u << (c - 1);
+        if (raw > half) { carry = 1; neg = true; return (1u << c) - raw; }
+        carry = 0; neg = false; return raw;
+    }
+};
+
+__global__ void k_count(const Fr* __restrict__ scalars, size_t n, uint32_t c, uint32_t W, uint32_t nb,
+                        bool shared, uint32_t* __restrict__ cnt)
+{
+    for (uint64_t i = gtid(); i < n; i += gstride()) {
+        DigitIter it; it.load(scalars + i);
+        for (uint32_t w = 0; w < W; w++) {
+            bool neg; uint32_t d = it.next(w, c, neg);
+            if (d) atomicAdd(cnt + (shared ? 0u : w * nb) + d - 1, 1u);
+        }
+    }
+}
+
+__global__ void k_scatter(const Fr* __restrict__ scalars, size_t n, uint32_t c, uint32_t W, uint32_t nb,
+                          bool shared, size_t stride, const uint32_t* __restrict__ off,
+                          uint32_t* __restrict__ cnt, uint32_t* __restrict__ ent)
+{
+    for (uint64_t i = gtid(); i < n; i += gstride()) {
+        DigitIter it; it.load(scalars + i);
+        for (uint32_t w = 0; w < W; w++) {
+            bool neg; uint32_t d = it.next(w, c, neg);
+            if (!d) continue;
+            uint32_t b = (shared ? 0u : w * nb) + d - 1;
+            uint32_t slot = off[b] + atomicSub(cnt + b, 1u) - 1u;
+            uint32_t idx = (uint32_t)(shared ? (size_t)w * stride + i : i);
+            ent[slot] = idx | (neg ? 0x80000000u : 0u);
+        }
+    }
+}
+
+// Exclusive scan of cnt[0..B) into off[0..B], off[B] = total.  One block of
+// 1024 threads; thread t owns a contiguous run of ceil(B/1024) counters.
+__global__ void __launch_bounds__(1024) k_scan(const uint32_t* __restrict__ cnt, uint32_t B, uint32_t* __restrict__ off)
+{
+    __shared__ uint32_t warp_tot[32];
+    uint32_t per = (B + 1023) / 1024;
+    uint32_t beg = threadIdx.x * per, end = min(beg + per, B);
+    uint32_t sum = 0;
+    for (uint32_t i = beg; i < end; i++) sum += cnt[i];
+    uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint32_t x = sum;
+    for (int o = 1; o < 32; o <<= 1) { uint32_t y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= (uint32_t)o) x += y; }
+    if (lane == 31) warp_tot[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        uint32_t t = warp_tot[lane];
+        for (int o = 1; o < 32; o <<= 1) { uint32_t y = __shfl_up_sync(0xffffffffu, t, o); if (lane >= (uint32_t)o) t += y; }
+        warp_tot[lane] = t;
+    }
+    __syncthreads();
+    uint32_t run = x - sum + (wid ? warp_tot[wid - 1] : 0u);
+    for (uint32_t i = beg; i < end; i++) { off[i] = run; run += cnt[i]; }
+    if (threadIdx.x == 1023) off[B] = warp_tot[31];
+}
+
+int msm_sort(const MsmPlan& p, const Fr* scalars, uint32_t* cnt, uint32_t* off, uint32_t* ent, cudaStream_t st)
+{
+    LZK_CUDA(cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * p.B, st));
+    unsigned g = grid_for(p.n, 256, 148 * 16);
+    k_count<<<g, 256, 0, st>>>(scalars, p.n, p.c, p.W, p.nb, p.shared, cnt);
+    k_scan<<<1, 1024, 0, st>>>(cnt, p.B, off);
+    k_scatter<<<g, 256, 0, st>>>(scalars, p.n, p.c, p.W, p.nb, p.shared, p.stride, off, cnt, ent);
+    return launch_status();
+}
+
+// Cost model behind the default window width: mixed adds n*W(c) (8M+2S) plus
+// the reduction (two XYZZ adds per bucket, 12M+2S) plus, for plain bases,
+// the serial Horner doublings, weighted by their latency cost.
+uint32_t msm_autotune(int group, size_t n, bool shared)
+{
+    (void)group;
+    if (n == 0) return 8;
+    double best = 1e300; uint32_t bc = 8;
+    for (uint32_t c = 4; c <= 22; c++) {
+        double W = windows_for(c);
+        double sets = shared ? 1.0 : W;
+        double cost = (double)n * W * 10.0 + sets * (double)(1u << (c - 1)) * 2.0 * 14.0;
+        if (!shared) cost += W * c * 9.0 * 2000.0;  // serial doublings are latency bound
+        if (shared && (double)n * W > 1.9e9) continue;
+        if (cost < best) { best = cost; bc = c; }
+    }
+    return bc;
+}
+
+}  // namespace lzk
+
+using namespace lzk;
+
+extern "C" {
+
+uint32_t lzk_msm_precomp_windows(uint32_t window_bits) { return window_bits ? windows_for(window_bits) : 0; }
+
+uint32_t lzk_msm_autotune_window(int group, size_t n, uint32_t flags)
+{
+    return msm_autotune(group, n, (flags & LZK_MSM_PRECOMPUTED) != 0);
+}
+
+size_t lzk_msm_workspace_bytes(int group, size_t n, const lzk_msm_cfg* cfg)
+{
+    bool shared = cfg && (cfg->flags & LZK_MSM_PRECOMPUTED);
+    uint32_t c = (cfg && cfg->window_bits) ? cfg->window_bits : msm_autotune(group, n, shared);
+    if (c < 2 || c > 24 || n == 0) return 0;
+    MsmPlan p;
+    if (group == 2) plan_msm<G2>(p, n, c, shared, cfg ? cfg->level_stride : 0);
+    else plan_msm<G1>(p, n, c, shared, cfg ? cfg->level_stride : 0);
+    return p.bytes;
+}
+
+}  // extern "C"

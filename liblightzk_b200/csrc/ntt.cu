@@ -1,0 +1,315 @@
+// ntt.cu -- number-theoretic transforms over BN254 Fr.
+//
+// Replaces number_theory_transformation and its kernels (reference
+// include/operator/poly.cuh:32-73): same transform, X_k = sum_j a_j w^(jk)
+// in natural order with w the 2^k-th root of unity of ntt-params.cuh
+// (w_k = w_28^(2^(28-k)), w_28 = 5^((r-1)/2^28)), and the same radix-2
+// decimation-in-frequency butterfly c[j] = lo + hi, c[j^h] = (lo - hi) *
+// w^((j mod h) << s).  Instead of one global-memory launch per stage, each
+// pass loads 2^m-element groups into shared memory and runs m stages there
+// (ceil(k / 11) passes for a size-2^k transform); a final pass applies the
+// bit-reversal permutation in place together with the scale n^-1 and the
+// coset factor.
+//
+// Directions: forward; inverse (w^-1, then * n^-1); coset forward (a_j *
+// g^j first, g = 5 = Fr::multiplicative_generator, alt_bn128_init.cu:50);
+// coset inverse (inverse, then * g^-j).
+#include "common.cuh"
+#include "field.cuh"
+#include <map>
+#include <mutex>
+
+namespace lzk {
+
+constexpr int kNttMaxLog = 26;
+constexpr uint32_t kNttElems = 2048;   // elements per block in a pass (64 KB smem)
+constexpr uint32_t kNttThreads = 256;
+constexpr uint32_t kPowLoBits = 12;    // g^j = lo[j & 4095] * hi[j >> 12]
+
+enum : uint32_t { NTT_PRE_COSET = 1u };
+
+// Montgomery form of w_28 = 5^((r-1)/2^28) and of g = 5
+__device__ __forceinline__ Fr root28()
+{
+    return Fr{{0x80d13d9cu, 0x636e7355u, 0x2445ffd6u, 0xa22bf374u, 0x1eb203d8u, 0x56452ac0u, 0x2963f9e7u, 0x1860ef94u}};
+}
+__device__ __forceinline__ Fr gen5()
+{
+    return Fr{{0x9fffffe6u, 0x1b0d0ef9u, 0xa32a913fu, 0xeaba68a3u, 0xd8dd0689u, 0x47d8eb76u, 0x20f5bbc3u, 0x15d00855u}};
+}
+
+__device__ __forceinline__ Fr fr_pow(Fr b, uint64_t e)
+{
+    Fr r = Fr::one();
+    while (e) {
+        if (e & 1) r = mul(r, b);
+        b = sqr(b);
+        e >>= 1;
+    }
+    return r;
+}
+
+// consts[0] = w_k, [1] = w_k^-1, [2] = 2^-k, [3] = g, [4] = g^-1,
+// [5] = g^(2^12), [6] = g^-(2^12)
+__global__ void k_ntt_consts(uint32_t k, Fr* consts)
+{
+    if (gtid() != 0) return;
+    Fr w = root28();
+    for (uint32_t i = k; i < 28; i++) w = sqr(w);
+    consts[0] = w;
+    consts[1] = inverse(w);
+    Fr two = add(Fr::one(), Fr::one());
+    consts[2] = inverse(fr_pow(two, k));
+    Fr g = gen5();
+    consts[3] = g;
+    consts[4] = inverse(g);
+    consts[5] = fr_pow(g, 1ull << kPowLoBits);
+    consts[6] = fr_pow(consts[4], 1ull << kPowLoBits);
+}
+
+// out[i] = base^i for i < count (64 consecutive powers per thread)
+__global__ void k_powers(const Fr* __restrict__ basep, Fr* __restrict__ out, size_t count)
+{
+    const uint32_t C = 64;
+    Fr base = *basep;
+    for (uint64_t t = gtid(); t * C < count; t += gstride()) {
+        size_t s = t * C;
+        Fr v = fr_pow(base, s);
+        size_t e = s + C < count ? s + C : count;
+        for (size_t i = s; i < e; i++) { st_elem(out + i, v); v = mul(v, base); }
+    }
+}
+
+struct NttTables {
+    Fr* tw[2] = {nullptr, nullptr};  // w^e, w^-e for e < n/2
+    Fr* consts = nullptr;            // see k_ntt_consts
+};
+
+struct CosetTables {
+    Fr* lo[2] = {nullptr, nullptr};  // g^j, g^-j for j < 4096
+    Fr* hi[2] = {nullptr, nullptr};  // g^(4096 i), g^-(4096 i) for i < 2^(26-12)
+};
+
+static std::mutex g_ntt_mu;
+static std::map<std::pair<int, uint32_t>, NttTables> g_ntt_tables;
+static std::map<int, CosetTables> g_coset_tables;
+
+// Build (once per device and size, synchronously, outside any stream
+// capture) the twiddle tables of a size-2^k transform.
+static int get_tables(uint32_t k, NttTables& out, CosetTables& cos)
+{
+    int dev;
+    LZK_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> g(g_ntt_mu);
+    auto it = g_ntt_tables.find({dev, k});
+    auto ct = g_coset_tables.find(dev);
+    if (it != g_ntt_tables.end() && ct != g_coset_tables.end()) { out = it->second; cos = ct->second; return LZK_OK; }
+    cudaStream_t st;
+    LZK_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    int rc = LZK_OK;
+    if (it == g_ntt_tables.end()) {
+        NttTables t;
+        size_t half = k ? (size_t(1) << (k - 1)) : 1;
+        if (cudaMalloc(&t.consts, 8 * sizeof(Fr)) != cudaSuccess || cudaMalloc(&t.tw[0], half * sizeof(Fr)) != cudaSuccess ||
+            cudaMalloc(&t.tw[1], half * sizeof(Fr)) != cudaSuccess) {
+            cudaGetLastError();
+            rc = LZK_ENOMEM;
+        } else {
+            k_ntt_consts<<<1, 32, 0, st>>>(k, t.consts);
+            k_powers<<<grid_for((half + 63) / 64, 128), 128, 0, st>>>(t.consts + 0, t.tw[0], half);
+            k_powers<<<grid_for((half + 63) / 64, 128), 128, 0, st>>>(t.consts + 1, t.tw[1], half);
+            rc = cuda_status(cudaStreamSynchronize(st));
+            if (rc == LZK_OK) g_ntt_tables[{dev, k}] = t;
+        }
+    }
+    if (rc == LZK_OK && ct == g_coset_tables.end()) {
+        CosetTables c;
+        size_t nlo = size_t(1) << kPowLoBits, nhi = size_t(1) << (kNttMaxLog - kPowLoBits);
+        Fr* cst = g_ntt_tables[{dev, k}].consts;
+        bool ok = true;
+        for (int d = 0; d < 2 && ok; d++)
+            ok = cudaMalloc(&c.lo[d], nlo * sizeof(Fr)) == cudaSuccess && cudaMalloc(&c.hi[d], nhi * sizeof(Fr)) == cudaSuccess;
+        if (!ok) { cudaGetLastError(); rc = LZK_ENOMEM; }
+        else {
+            for (int d = 0; d < 2; d++) {
+                k_powers<<<grid_for(nlo / 64, 128), 128, 0, st>>>(cst + 3 + d, c.lo[d], nlo);
+                k_powers<<<grid_for(nhi / 64, 128), 128, 0, st>>>(cst + 5 + d, c.hi[d], nhi);
+            }
+            rc = cuda_status(cudaStreamSynchronize(st));
+            if (rc == LZK_OK) g_coset_tables[dev] = c;
+        }
+    }
+    cudaStreamDestroy(st);
+    if (rc != LZK_OK) return rc;
+    out = g_ntt_tables[{dev, k}];
+    cos = g_coset_tables[dev];
+    return LZK_OK;
+}
+
+struct NttPass {
+    uint32_t k, s0, m, lowbits, R;
+};
+
+__device__ __forceinline__ Fr coset_pow(const Fr* lo, const Fr* hi, size_t j)
+{
+    return mul(ldg_elem(lo + (j & ((1u << kPowLoBits) - 1))), ldg_elem(hi + (j >> kPowLoBits)));
+}
+
+// m DIF stages s0..s0+m-1 over groups of 2^m elements that differ in index
+// bits [lowbits, lowbits+m); R groups with consecutive (outer, low) index
+// per block.  `batch` transforms of size 2^k lie `bstride` elements apart.
+__global__ void __launch_bounds__(kNttThreads) k_ntt_pass(Fr* __restrict__ data, NttPass p, const Fr* __restrict__ tw,
+                                                           uint32_t flags, const Fr* __restrict__ clo,
+                                                           const Fr* __restrict__ chi, size_t bstride)
+{
+    extern __shared__ uint4 smem_raw[];
+    Fr* sm = reinterpret_cast<Fr*>(smem_raw);
+    Fr* d = data + (size_t)blockIdx.y * bstride;
+    const uint32_t G = 1u << p.m, R = p.R;
+    const uint32_t rbits = __ffs(R) - 1;
+    const size_t lowmask = (size_t(1) << p.lowbits) - 1;
+    const uint32_t tot = G * R;
+    for (uint32_t i = threadIdx.x; i < tot; i += blockDim.x) {
+        uint32_t g = i >> rbits, r = i & (R - 1);
+        size_t cidx = (size_t)blockIdx.x * R + r;
+        size_t j = ((cidx >> p.lowbits) << (p.k - p.s0)) | ((size_t)g << p.lowbits) | (cidx & lowmask);
+        Fr x = ldg_elem(d + j);
+        if (flags & NTT_PRE_COSET) x = mul(x, coset_pow(clo, chi, j));
+        st_elem(sm + i, x);
+    }
+    __syncthreads();
+    for (uint32_t t = 0; t < p.m; t++) {
+        uint32_t hb = p.m - 1 - t;        // half = 2^hb groups
+        uint32_t s = p.s0 + t;
+        for (uint32_t b = threadIdx.x; b < tot / 2; b += blockDim.x) {
+            uint32_t r = b & (R - 1), gb = b >> rbits;
+            uint32_t g = ((gb >> hb) << (hb + 1)) | (gb & ((1u << hb) - 1));
+            uint32_t i0 = (g << rbits) | r, i1 = ((g + (1u << hb)) << rbits) | r;
+            size_t low = ((size_t)blockIdx.x * R + r) & lowmask;
+            size_t e = ((((size_t)(g & ((1u << hb) - 1))) << p.lowbits) | low) << s;
+            Fr lo = ld_elem(sm + i0), hi = ld_elem(sm + i1);
+            st_elem(sm + i0, add(lo, hi));
+            st_elem(sm + i1, mul(sub(lo, hi), ldg_elem(tw + e)));
+        }
+        __syncthreads();
+    }
+    for (uint32_t i = threadIdx.x; i < tot; i += blockDim.x) {
+        uint32_t g = i >> rbits, r = i & (R - 1);
+        size_t cidx = (size_t)blockIdx.x * R + r;
+        size_t j = ((cidx >> p.lowbits) << (p.k - p.s0)) | ((size_t)g << p.lowbits) | (cidx & lowmask);
+        st_elem(d + j, ld_elem(sm + i));
+    }
+}
+
+__device__ __forceinline__ size_t brev_k(size_t j, uint32_t k)
+{
+    return (size_t)(__brevll((unsigned long long)j) >> (64 - k));
+}
+
+// In-place bit reversal; each output position pos is then multiplied by
+// scale (when non-null) and g^-pos (when clo != null).
+__global__ void k_ntt_bitrev(Fr* __restrict__ data, uint32_t k, const Fr* __restrict__ scale,
+                             const Fr* __restrict__ clo, const Fr* __restrict__ chi, size_t bstride)
+{
+    Fr* d = data + (size_t)blockIdx.y * bstride;
+    size_t n = size_t(1) << k;
+    Fr sc = scale ? ldg_elem(scale) : Fr::one();
+    for (uint64_t j = gtid(); j < n; j += gstride()) {
+        size_t r = k ? brev_k(j, k) : 0;
+        if (j > r) continue;
+        Fr a = ld_elem(d + j), b = ld_elem(d + r);
+        // after the swap position j holds b and position r holds a
+        if (scale) { a = mul(a, sc); if (j != r) b = mul(b, sc); }
+        if (clo) { a = mul(a, coset_pow(clo, chi, r)); if (j != r) b = mul(b, coset_pow(clo, chi, j)); }
+        st_elem(d + r, a);
+        if (j != r) st_elem(d + j, b);
+    }
+}
+
+// Enqueue the passes of `count` transforms of size 2^k (natural order in,
+// natural order out) with twiddle table tw (w^e, e < n/2).
+static int ntt_enqueue(Fr* data, uint32_t k, uint32_t count, size_t bstride, const Fr* tw, const Fr* scale,
+                       const Fr* pre_lo, const Fr* pre_hi, const Fr* post_lo, const Fr* post_hi, cudaStream_t st)
+{
+    static bool attr_set[64] = {false};
+    int dev = 0;
+    LZK_CUDA(cudaGetDevice(&dev));
+    if (dev < 64 && !attr_set[dev]) {
+        LZK_CUDA(cudaFuncSetAttribute(k_ntt_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttElems * sizeof(Fr)));
+        attr_set[dev] = true;
+    }
+    if (k == 0) {
+        if (scale || post_lo || pre_lo) {
+            k_ntt_bitrev<<<dim3(1, count), 32, 0, st>>>(data, 0, scale, post_lo, post_hi, bstride);
+            return launch_status();
+        }
+        return LZK_OK;
+    }
+    uint32_t maxm = 11;
+    uint32_t P = (k + maxm - 1) / maxm;
+    size_t n = size_t(1) << k;
+    uint32_t s0 = 0;
+    for (uint32_t q = 0; q < P; q++) {
+        uint32_t m = (k - s0) / (P - q);      // balanced split, larger passes last
+        NttPass pp;
+        pp.k = k; pp.s0 = s0; pp.m = m; pp.lowbits = k - s0 - m;
+        uint32_t G = 1u << m;
+        uint32_t R = kNttElems / G;
+        if ((size_t)R > (n >> m)) R = (uint32_t)(n >> m);
+        if (R == 0) R = 1;
+        pp.R = R;
+        size_t blocks = (n >> m) / R;
+        size_t smem = (size_t)G * R * sizeof(Fr);
+        uint32_t flags = (q == 0 && pre_lo) ? NTT_PRE_COSET : 0u;
+        k_ntt_pass<<<dim3((unsigned)blocks, count), kNttThreads, smem, st>>>(data, pp, tw, flags, pre_lo, pre_hi, bstride);
+        s0 += m;
+    }
+    k_ntt_bitrev<<<dim3(grid_for(n, 256, 148 * 8), count), 256, 0, st>>>(data, k, scale, post_lo, post_hi, bstride);
+    return launch_status();
+}
+
+static int run_ntt(Fr* data, uint32_t k, int dir, uint32_t count, size_t bstride, cudaStream_t st)
+{
+    if (!data || k > kNttMaxLog || dir < 0 || dir > 3 || count == 0 || count > 65535) return LZK_EINVAL;
+    if (count > 1 && bstride < (size_t(1) << k)) return LZK_EINVAL;
+    NttTables t; CosetTables c;
+    LZK_TRY(get_tables(k, t, c));
+    bool inv = dir & 1, coset = dir >= 2;
+    return ntt_enqueue(data, k, count, bstride, t.tw[inv ? 1 : 0], inv ? t.consts + 2 : nullptr,
+                       (coset && !inv) ? c.lo[0] : nullptr, (coset && !inv) ? c.hi[0] : nullptr,
+                       (coset && inv) ? c.lo[1] : nullptr, (coset && inv) ? c.hi[1] : nullptr, st);
+}
+
+}  // namespace lzk
+
+using namespace lzk;
+
+extern "C" {
+
+int lzk_ntt_prepare(uint32_t log_n)
+{
+    if (log_n > kNttMaxLog) return LZK_EINVAL;
+    NttTables t; CosetTables c;
+    return get_tables(log_n, t, c);
+}
+
+int lzk_ntt(lzk_fr_t* data, uint32_t log_n, int direction, void* stream)
+{
+    return run_ntt(reinterpret_cast<Fr*>(data), log_n, direction, 1, 0, as_stream(stream));
+}
+
+int lzk_ntt_batch(lzk_fr_t* data, uint32_t log_n, uint32_t count, size_t stride, int direction, void* stream)
+{
+    return run_ntt(reinterpret_cast<Fr*>(data), log_n, direction, count, stride, as_stream(stream));
+}
+
+int lzk_number_theory_transformation(size_t deg, size_t log_deg, lzk_fr_t* coeffs, const lzk_fr_t* omega_powers,
+                                     const lzk_fr_t* factor, void* stream)
+{
+    if (!coeffs || !omega_powers || log_deg > 30 || deg != (size_t(1) << log_deg)) return LZK_EINVAL;
+    return ntt_enqueue(reinterpret_cast<Fr*>(coeffs), (uint32_t)log_deg, 1, 0,
+                       reinterpret_cast<const Fr*>(omega_powers), reinterpret_cast<const Fr*>(factor),
+                       nullptr, nullptr, nullptr, nullptr, as_stream(stream));
+}
+
+}  // extern "C"
