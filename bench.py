@@ -1,0 +1,359 @@
+#!/usr/bin/env python
+"""Groth16 prover benchmark on B200: proofs/s and p50/p99 latency at 2^20
+constraints, plus the G1 MSM at 2^20 in ms.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one Groth16 proof of the synthetic 2^20-constraint circuit (a
+fresh witness per step, alternating among pre-solved witnesses), through
+lzk_groth16_prove.  `value` is whole-job proofs/s with the witness already
+in HBM; `e2e` adds, every step, the host->device copy of that step's witness
+from pinned memory and the device->host read of the proof.  With N > 1 each
+rank is an independent replica (proofs do not shard) and the slowest rank's
+time is used.  `--impl reference` times the reference's own CPU path (the
+libff-derived host arithmetic built into oracle/_ref) on a bounded sample
+and extrapolates to one proof.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Groth16 proofs/s & p50/p99 latency at 2^20 constraints; G1 MSM 2^20 ms"
+IMAD_PER_FP_MUL = 264          # 8x8 lo + 8x8 hi products, 8 x (1 + 8 + 8) reduction
+FP_MUL_PER_G1_MADD = 10        # XYZZ mixed addition: 8M + 2S
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--log-m", type=int, default=20)
+    ap.add_argument("--mode", choices=["standard", "reference"], default="standard")
+    ap.add_argument("--window", type=int, default=16)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during a region"""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for n, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# --------------------------------------------------------------- CPU side
+def cpu_reference_sample(log_m, n_vars, n_l, seed=3):
+    """Time the reference's own CPU path (oracle/_ref: libff-derived host
+    arithmetic) on a bounded sample and extrapolate to one 2^log_m proof:
+    the naive MSM of test/msm-check.cu:45-55 (OpenMP over all cores) per G1
+    and G2 point, the reference's radix-2 NTT (poly.cuh:32-73 restated on
+    libff Fr) per butterfly, and the CSR SpMV per row.  Returns a dict."""
+    from oracle import FR, Oracle, Ref, have_ref
+    orc = Oracle()
+    lib = Ref() if have_ref() else None
+    kind = "reference" if lib else "port"
+    L = lib if lib else orc
+    st = np.array([seed], np.uint64)
+    M = 1 << log_m
+    n1, n2, nt = 1 << 13, 1 << 11, 1 << 16
+    k = orc.rand_field(FR, n1, st)
+    jac1 = orc.aff_to_jac(1, orc.fixed_base(1, k))
+    jac2 = orc.aff_to_jac(2, orc.fixed_base(2, k[:n2]))
+    s = orc.rand_field(FR, n1, st)
+    t0 = time.perf_counter()
+    if lib:
+        lib.g1_msm_naive_jac(s, jac1)
+    else:
+        orc.msm(1, s, orc.jac_to_aff(1, jac1), naive=True)
+    t_g1 = (time.perf_counter() - t0) / n1
+    t0 = time.perf_counter()
+    if lib:
+        lib.g2_msm_naive_jac(s[:n2], jac2)
+    else:
+        orc.msm(2, s[:n2], orc.jac_to_aff(2, jac2), naive=True)
+    t_g2 = (time.perf_counter() - t0) / n2
+    tab = L.ntt_setup(nt)
+    c = orc.rand_field(FR, nt, st)
+    t0 = time.perf_counter()
+    L.ntt_ref(c, tab[nt:2 * nt], tab[2 * nt])
+    t_bfly = (time.perf_counter() - t0) / ((nt // 2) * 16)
+    # reference chain: 3 iNTT_M + 3 NTT_2M + 1 iNTT_2M (groth16.cuh:166-185)
+    bfly = 3 * (M // 2) * log_m + 4 * M * (log_m + 1)
+    rows = 1 << 14
+    per = np.full(rows, 2, np.int64)
+    rp = np.concatenate([[0], np.cumsum(per)[:-1]]).astype(np.uint64)
+    col = np.random.default_rng(1).integers(0, rows, 2 * rows).astype(np.uint64)
+    val = orc.rand_field(FR, 2 * rows, st)
+    z = orc.rand_field(FR, rows, st)
+    t0 = time.perf_counter()
+    L.spmv(val, col, rp, z) if lib else orc.spmv(val, col, rp, z)
+    t_row = (time.perf_counter() - t0) / rows
+    t_proof = (2 * n_vars + n_l + (M - 1)) * t_g1 + n_vars * t_g2 + bfly * t_bfly + 3 * M * t_row
+    return {"value": 1.0 / t_proof, "unit": "proofs/s", "cores": os.cpu_count(), "kind": kind,
+            "sample": (f"naive MSM (test/msm-check.cu:45-55, OpenMP) on {n1} G1 and {n2} G2 points, "
+                       f"radix-2 NTT of 2^16 and SpMV of {rows} rows, extrapolated to one 2^{log_m} proof "
+                       f"(4 G1 MSMs + 1 G2 MSM over {n_vars} variables, 7 NTTs, 3 SpMVs)"),
+            "seconds_per_proof": t_proof, "per_point_us": {"g1": t_g1 * 1e6, "g2": t_g2 * 1e6}}
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    M = 1 << args.log_m
+    n_vars = M + 4096 + 2
+    vals = []
+    for _ in range(args.warmup):
+        cpu_reference_sample(min(args.log_m, 12), n_vars, n_vars - 2)
+    t_start = time.perf_counter()
+    for i in range(args.steps):
+        vals.append(cpu_reference_sample(args.log_m, n_vars, n_vars - 2, seed=3 + i))
+    wall = time.perf_counter() - t_start
+    v = float(np.mean([x["value"] for x in vals]))
+    cb = dict(vals[-1])
+    cb["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "proofs/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (Fr/Fq mod p)",
+            "data": "synthetic", "config": {"workload": f"groth16_prove_2^{args.log_m}", "constraints": M,
+                                            "variables": n_vars, "sample": "bounded CPU sample per step"},
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": "proofs/s", "h2d_bytes_per_step": 0,
+                                         "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------- GPU side
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    from liblightzk_b200 import _capi, device, groth16, msm, synth
+    dev = f"cuda:{local}"
+    log_m = args.log_m
+    M = 1 << log_m
+
+    # ---------------- setup (untimed) ----------------
+    circ = synth.Circuit(log_m, seed=1, device=dev)
+    pk = synth.ProvingKey(circ, seed=7)
+    mode = groth16.STANDARD if args.mode == "standard" else groth16.REFERENCE
+    prover = groth16.Prover(circ, pk, mode=mode, window_bits=args.window)
+    nw = 2
+    wits = [circ.witness(100 + rank * 10 + i) for i in range(nw)]
+    host_wits = [device.to_host(w) for w in wits]
+    pinned = [torch.from_numpy(h.view(np.int64)).pin_memory() for h in host_wits]
+    nsteps = args.warmup + args.steps
+    rs = device.to_host(synth.random_fr(2 * nsteps, 9 + rank, 99, device=dev)).reshape(nsteps, 2, 4)
+    proofs = torch.empty((nsteps, groth16.PROOF_WORDS), dtype=torch.int64, device=dev)
+    torch.cuda.synchronize()
+
+    def step(i, z):
+        prover.prove(z, rs[i, 0], rs[i, 1], proof=proofs[i])
+
+    for i in range(args.warmup):
+        step(i, wits[i % nw])
+    torch.cuda.synchronize()
+
+    # ---------------- timed: device-resident inputs ----------------
+    clocks = Clocks(local)
+    clocks.start()
+    _capi.trace_reset()
+    _capi.trace_enable(True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(args.steps):
+        ev[k][0].record()
+        step(args.warmup + k, wits[k % nw])
+        ev[k][1].record()
+    e1.record()
+    torch.cuda.synchronize()
+    _capi.trace_enable(False)
+    ms_total = e0.elapsed_time(e1)
+    lat = sorted(a.elapsed_time(b) for a, b in ev)
+    acc_ms, acc_n = _capi.trace_get("msm_g1_accumulate")
+    acc2_ms, acc2_n = _capi.trace_get("msm_g2_accumulate")
+    msm1_ms, msm1_n = _capi.trace_get("msm_g1")
+    msm2_ms, msm2_n = _capi.trace_get("msm_g2")
+    clk = clocks.stop()
+
+    # ---------------- timed: end to end through host memory ----------------
+    zdev = torch.empty_like(wits[0])
+    host_proofs = torch.empty((args.steps, groth16.PROOF_WORDS), dtype=torch.int64).pin_memory()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record()
+    for k in range(args.steps):
+        zdev.copy_(pinned[k % nw], non_blocking=True)
+        p = prover.prove(zdev, rs[args.warmup + k, 0], rs[args.warmup + k, 1], proof=proofs[args.warmup + k])
+        host_proofs[k].copy_(p, non_blocking=True)
+    f1.record()
+    torch.cuda.synchronize()
+    e2e_ms = f0.elapsed_time(f1)
+
+    # max over ranks
+    if dist:
+        t = torch.tensor([ms_total, e2e_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total, e2e_ms = float(t[0]), float(t[1])
+
+    # ---------------- G1 MSM at 2^20 (precomputed table, as msm-check.cu) ----------------
+    g1_ms = g1_plain_ms = None
+    if rank == 0:
+        n = 1 << 20
+        sc = synth.random_fr(n, 5, 77, device=dev)
+        bases = pk.a[:n] if pk.a.shape[0] >= n else synth.fixed_base(1, synth.random_fr(n, 5, 78, device=dev))
+        c = args.window
+        W = msm.windows_for(c)
+        table = msm.precompute(1, bases, c, W, n)
+        ws = torch.empty(msm.workspace_bytes(1, n, c, True, n), dtype=torch.uint8, device=dev)
+        times = []
+        for it in range(8):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            msm.msm_precomputed(1, sc, table, c, W, n, workspace=ws)
+            b.record()
+            torch.cuda.synchronize()
+            if it >= 3:
+                times.append(a.elapsed_time(b))
+        g1_ms = float(np.median(times))
+        del table
+        times = []
+        for it in range(5):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            msm.msm(1, sc, bases)
+            b.record()
+            torch.cuda.synchronize()
+            if it >= 2:
+                times.append(a.elapsed_time(b))
+        g1_plain_ms = float(np.median(times))
+
+    if dist:
+        dist.barrier()
+    if rank != 0:
+        dist.destroy_process_group()
+        return
+
+    # ---------------- roofline of the dominant kernel ----------------
+    imad_peak = _capi.probe_imad_rate()
+    W = msm.windows_for(args.window)
+    nl = circ.n_vars - circ.n_public - 1
+    g1_points_per_proof = 2 * circ.n_vars + nl + (M - 1)
+    g1_launches_per_proof = 4
+    avg_pts = g1_points_per_proof / g1_launches_per_proof
+    alg_imad = avg_pts * W * FP_MUL_PER_G1_MADD * IMAD_PER_FP_MUL
+    acc_avg_ms = acc_ms / max(acc_n, 1)
+    achieved = alg_imad / (acc_avg_ms * 1e-3) if acc_n else None
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "msm_g1_accumulate_traffic.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get("bytes_per_launch_at_2e20")
+        except Exception:
+            traffic = None
+
+    proofs_s = world * args.steps / (ms_total * 1e-3)
+    line = {
+        "metric": METRIC, "value": proofs_s, "unit": "proofs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (Fr/Fq mod p, Montgomery)",
+        "data": "synthetic (seeded R1CS, witness and proving key generated on the device)",
+        "config": {"workload": f"groth16_prove_2^{log_m}", "constraints": M, "variables": circ.n_vars,
+                   "public_inputs": circ.n_public, "prove_mode": args.mode, "msm_window_bits": args.window,
+                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (GB-scale key tables)"},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "mean": float(np.mean(lat))},
+        "g1_msm_2e20_ms": g1_ms, "g1_msm_2e20_plain_ms": g1_plain_ms,
+        "e2e": {"value": world * args.steps / (e2e_ms * 1e-3), "unit": "proofs/s",
+                "h2d_bytes_per_step": int(wits[0].numel() * 8), "d2h_bytes_per_step": groth16.PROOF_WORDS * 8},
+        "gpu_launches": None,
+        "roofline": {"kernel": "k_accumulate<Fq> (G1 bucket accumulation)", "bound": "int",
+                     "achieved": achieved / 1e12 if achieved else None, "peak": imad_peak / 1e12,
+                     "unit": "T IMAD/s", "frac": (achieved / imad_peak) if achieved else None,
+                     "traffic": traffic, "peak_source": "measured (lzk_probe_imad_rate, mad.lo/madc.hi chains)",
+                     "algorithmic_imad_per_launch": alg_imad, "avg_launch_ms": acc_avg_ms,
+                     "launches": acc_n},
+        "breakdown_ms_per_proof": {"msm_g1": msm1_ms / args.steps, "msm_g2": msm2_ms / args.steps,
+                                   "msm_g1_accumulate": acc_ms / args.steps,
+                                   "msm_g2_accumulate": acc2_ms / args.steps},
+        "clocks": clk,
+    }
+    if not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_reference_sample(log_m, circ.n_vars, nl)
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

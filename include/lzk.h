@@ -155,6 +155,95 @@ int lzk_spmv3(const lzk_csr* A, const lzk_csr* B, const lzk_csr* C, const lzk_fr
               lzk_fr_t* Az, lzk_fr_t* Bz, lzk_fr_t* Cz, void* stream);
 int lzk_spmv(const lzk_csr* M, const lzk_fr_t* z, lzk_fr_t* out, void* stream);
 
+/* ------------------------------------------------------------ setup path
+ * Seeded uniform Fr vector: out[i] is element offset+i of stream
+ * (seed, stream_id), drawn like Fp_model::random_element (fp.cuh:789-816)
+ * and used as Montgomery limbs.  Deterministic for equal arguments. */
+int lzk_random_fr(uint64_t seed, uint64_t stream_id, uint64_t offset, size_t n, lzk_fr_t* out, void* stream);
+/* Fixed-base products out[i] = k[i] * G (G the group generator of
+ * alt_bn128_init.cu:130-132 / 191-195), affine.  Replaces
+ * fix_base_multi_scalar_multiplication_g1/_g2 (msm.cuh:5-46). */
+int lzk_g1_fixed_base(const lzk_fr_t* k, size_t n, lzk_g1_affine_t* out, void* stream);
+int lzk_g2_fixed_base(const lzk_fr_t* k, size_t n, lzk_g2_affine_t* out, void* stream);
+/* Witness solving for circuits whose row i of C starts with the variable it
+ * defines (coefficient one): z[def_i] = (A_i z)(B_i z) - (rest of C_i z),
+ * for rows [row_begin, row_end), which may only read variables defined by
+ * earlier calls. */
+int lzk_r1cs_solve(const lzk_csr* A, const lzk_csr* B, const lzk_csr* C, lzk_fr_t* z, uint64_t row_begin,
+                   uint64_t row_end, void* stream);
+/* *bad_rows (device) = number of rows with (A_i z)(B_i z) != C_i z. */
+int lzk_r1cs_check(const lzk_csr* A, const lzk_csr* B, const lzk_csr* C, const lzk_fr_t* z,
+                   unsigned long long* bad_rows, void* stream);
+
+/* --------------------------------------------------------------- Groth16
+ * Replaces Groth16<...>::Prove (groth16.cuh:154-222).  A prover holds the
+ * circuit view, the proving key as resident shifted-copy MSM tables and its
+ * scratch; lzk_groth16_prove enqueues one proof on `stream` (internally
+ * forked onto two more streams and joined back) with no host round trip.
+ * One proof at a time per prover: calls on different streams must be
+ * ordered by the caller.
+ *
+ * mode LZK_PROVE_REFERENCE reproduces the reference chain bit for bit: the
+ * 2M-point H path with the (4M)^-1 scale of groth16-operator.cuh:13 and H
+ * scalars taken from coefficients M+1..2M-1 (groth16.cuh:168-198).
+ * mode LZK_PROVE_STANDARD computes the standard quotient h on the coset
+ * 5*<w_M> with size-M transforms and uses h_0..h_{M-2}.
+ * Phase 6 (groth16.cuh:211-215) runs on the device. */
+#define LZK_PROVE_STANDARD  0
+#define LZK_PROVE_REFERENCE 1
+
+typedef struct lzk_groth16_circuit {
+    lzk_csr A, B, C;          /* device CSR; rows = constraints <= 2^log_domain */
+    uint64_t n_vars;          /* N + 1 (z[0] = 1) */
+    uint64_t n_public;        /* k: the L query covers z[k+1 .. N] */
+    uint32_t log_domain;      /* M = 2^log_domain, 1..24 */
+    uint32_t reserved;
+} lzk_groth16_circuit;
+
+typedef struct lzk_groth16_pk {
+    const lzk_g1_affine_t* a_query;   /* device, n_vars points       (a1)  */
+    const lzk_g1_affine_t* b1_query;  /* device, n_vars               (b1)  */
+    const lzk_g2_affine_t* b2_query;  /* device, n_vars               (b2)  */
+    const lzk_g1_affine_t* l_query;   /* device, n_vars - n_public - 1 (Kpk) */
+    const lzk_g1_affine_t* h_query;   /* device, M - 1                (Z1)  */
+    lzk_g1_affine_t alpha1, beta1, delta1;   /* host values */
+    lzk_g2_affine_t beta2, delta2;
+} lzk_groth16_pk;
+
+typedef struct lzk_groth16_proof {
+    lzk_g1_t A;   /* Ar */
+    lzk_g2_t B;   /* Bs2 */
+    lzk_g1_t C;   /* Krs + HZ */
+} lzk_groth16_proof;
+
+typedef struct lzk_prover lzk_prover;
+
+/* window_bits: MSM window of the resident tables (0 = 16).  The query
+ * arrays of pk are read only during creation; the circuit's CSR arrays must
+ * stay valid while the prover lives. */
+int lzk_prover_create(const lzk_groth16_circuit* circuit, const lzk_groth16_pk* pk, int mode,
+                      uint32_t window_bits, lzk_prover** out);
+int lzk_prover_destroy(lzk_prover* prover);
+size_t lzk_prover_device_bytes(const lzk_prover* prover);
+/* z: device witness (n_vars Fr); r, s: HOST Fr values (Montgomery);
+ * proof: device memory. */
+int lzk_groth16_prove(lzk_prover* prover, const lzk_fr_t* z, const lzk_fr_t* r, const lzk_fr_t* s,
+                      lzk_groth16_proof* proof, void* stream);
+
+/* ------------------------------------------------------------ tracing
+ * Opt-in CUDA-event timing of named device regions ("msm_g1",
+ * "msm_g1_accumulate", "msm_g2", "msm_g2_accumulate", "groth16_prove").
+ * Replaces the reference's synchronising Timer/CUDA_DEBUG pairs
+ * (timer.cu:3-16, device-utils.cuh:3). */
+void lzk_trace_enable(int on);
+void lzk_trace_reset(void);
+/* Total device milliseconds and count of completed regions named `name`
+ * since the last reset (waits for pending regions). */
+int lzk_trace_get(const char* name, double* total_ms, uint64_t* count);
+/* Measured 32-bit integer multiply-add rate of the current device
+ * (mad.lo/madc.hi operations per second); synchronous. */
+int lzk_probe_imad_rate(double* ops_per_s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -33,6 +33,19 @@ SIGNATURES = {
     "lzk_number_theory_transformation": (c_i, [c_sz, c_sz, c_p, c_p, c_p, c_p]),
     "lzk_spmv3": (c_i, [c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_p]),
     "lzk_spmv": (c_i, [c_p, c_p, c_p, c_p]),
+    "lzk_random_fr": (c_i, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, c_sz, c_p, c_p]),
+    "lzk_g1_fixed_base": (c_i, [c_p, c_sz, c_p, c_p]),
+    "lzk_g2_fixed_base": (c_i, [c_p, c_sz, c_p, c_p]),
+    "lzk_r1cs_solve": (c_i, [c_p, c_p, c_p, c_p, ctypes.c_uint64, ctypes.c_uint64, c_p]),
+    "lzk_r1cs_check": (c_i, [c_p, c_p, c_p, c_p, c_p, c_p]),
+    "lzk_prover_create": (c_i, [c_p, c_p, c_i, c_u32, c_p]),
+    "lzk_prover_destroy": (c_i, [c_p]),
+    "lzk_prover_device_bytes": (c_sz, [c_p]),
+    "lzk_groth16_prove": (c_i, [c_p, c_p, c_p, c_p, c_p, c_p]),
+    "lzk_trace_enable": (None, [c_i]),
+    "lzk_trace_reset": (None, []),
+    "lzk_trace_get": (c_i, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64)]),
+    "lzk_probe_imad_rate": (c_i, [ctypes.POINTER(ctypes.c_double)]),
 }
 
 
@@ -103,3 +116,24 @@ def check(status, where=""):
 def call(name, *args):
     """Call an int-status entry point and raise LzkError on failure."""
     return check(getattr(lib(), name)(*args), name)
+
+
+def trace_enable(on=True):
+    lib().lzk_trace_enable(1 if on else 0)
+
+
+def trace_reset():
+    lib().lzk_trace_reset()
+
+
+def trace_get(name):
+    """(total device ms, count) of completed regions named `name`"""
+    ms, cnt = ctypes.c_double(), ctypes.c_uint64()
+    call("lzk_trace_get", name.encode(), ctypes.byref(ms), ctypes.byref(cnt))
+    return ms.value, cnt.value
+
+
+def probe_imad_rate():
+    r = ctypes.c_double()
+    call("lzk_probe_imad_rate", ctypes.byref(r))
+    return r.value

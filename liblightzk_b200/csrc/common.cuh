@@ -35,6 +35,12 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 
 inline size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
 
+// Opt-in event tracing of named device regions (trace.cu): a no-op returning
+// nullptr unless lzk_trace_enable(1) was called.
+bool trace_on();
+void* trace_begin(const char* name, cudaStream_t st);
+void trace_end(void* h, cudaStream_t st);
+
 // Make the current device's default memory pool keep freed blocks, so the
 // stream-ordered scratch of repeated calls is served from the pool.
 void keep_pool_cached();

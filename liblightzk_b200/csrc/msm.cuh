@@ -196,6 +196,7 @@ int run_msm(const Fr* scalars, const Aff<typename Gp::F>* bases, size_t n, Jac<t
     }
     MsmPlan p;
     plan_msm<Gp>(p, n, c, shared, stride);
+    void* tr_all = trace_begin(sizeof(F) == 32 ? "msm_g1" : "msm_g2", st);
     Scratch ws;
     LZK_TRY(ws.acquire(p.bytes, cfg ? cfg->workspace : nullptr, cfg ? cfg->workspace_bytes : 0, st));
     char* base = ws.base;
@@ -209,7 +210,9 @@ int run_msm(const Fr* scalars, const Aff<typename Gp::F>* bases, size_t n, Jac<t
     X* la[2] = {reinterpret_cast<X*>(base + p.o_la0), reinterpret_cast<X*>(base + p.o_la1)};
 
     LZK_TRY(msm_sort(p, scalars, cnt, off, ent, st));
+    void* tr = trace_begin(sizeof(F) == 32 ? "msm_g1_accumulate" : "msm_g2_accumulate", st);
     k_accumulate<F><<<grid_for(p.chunks, 256), 256, 0, st>>>(bases, ent, off, p.B, p.chunks, bsum, head, tail);
+    trace_end(tr, st);
     k_fixup<F><<<grid_for(p.B, 256, 148 * 8), 256, 0, st>>>(off, p.B, bsum, head, tail);
     LZK_TRY(launch_status());
 
@@ -231,6 +234,7 @@ int run_msm(const Fr* scalars, const Aff<typename Gp::F>* bases, size_t n, Jac<t
         if (m == 1) break;
     }
     k_finish<F><<<1, 32, 0, st>>>(resA, p.wb, c, out);
+    trace_end(tr_all, st);
     return launch_status();
 }
 

@@ -14,8 +14,7 @@
 // Directions: forward; inverse (w^-1, then * n^-1); coset forward (a_j *
 // g^j first, g = 5 = Fr::multiplicative_generator, alt_bn128_init.cu:50);
 // coset inverse (inverse, then * g^-j).
-#include "common.cuh"
-#include "field.cuh"
+#include "ntt.cuh"
 #include <map>
 #include <mutex>
 
@@ -80,23 +79,13 @@ __global__ void k_powers(const Fr* __restrict__ basep, Fr* __restrict__ out, siz
     }
 }
 
-struct NttTables {
-    Fr* tw[2] = {nullptr, nullptr};  // w^e, w^-e for e < n/2
-    Fr* consts = nullptr;            // see k_ntt_consts
-};
-
-struct CosetTables {
-    Fr* lo[2] = {nullptr, nullptr};  // g^j, g^-j for j < 4096
-    Fr* hi[2] = {nullptr, nullptr};  // g^(4096 i), g^-(4096 i) for i < 2^(26-12)
-};
-
 static std::mutex g_ntt_mu;
 static std::map<std::pair<int, uint32_t>, NttTables> g_ntt_tables;
 static std::map<int, CosetTables> g_coset_tables;
 
 // Build (once per device and size, synchronously, outside any stream
 // capture) the twiddle tables of a size-2^k transform.
-static int get_tables(uint32_t k, NttTables& out, CosetTables& cos)
+int get_tables(uint32_t k, NttTables& out, CosetTables& cos)
 {
     int dev;
     LZK_CUDA(cudaGetDevice(&dev));
@@ -268,14 +257,15 @@ static int ntt_enqueue(Fr* data, uint32_t k, uint32_t count, size_t bstride, con
     return launch_status();
 }
 
-static int run_ntt(Fr* data, uint32_t k, int dir, uint32_t count, size_t bstride, cudaStream_t st)
+int ntt_run(Fr* data, uint32_t k, int dir, uint32_t count, size_t bstride, const Fr* scale_override, cudaStream_t st)
 {
     if (!data || k > kNttMaxLog || dir < 0 || dir > 3 || count == 0 || count > 65535) return LZK_EINVAL;
     if (count > 1 && bstride < (size_t(1) << k)) return LZK_EINVAL;
     NttTables t; CosetTables c;
     LZK_TRY(get_tables(k, t, c));
     bool inv = dir & 1, coset = dir >= 2;
-    return ntt_enqueue(data, k, count, bstride, t.tw[inv ? 1 : 0], inv ? t.consts + 2 : nullptr,
+    const Fr* scale = scale_override ? scale_override : (inv ? t.consts + 2 : nullptr);
+    return ntt_enqueue(data, k, count, bstride, t.tw[inv ? 1 : 0], scale,
                        (coset && !inv) ? c.lo[0] : nullptr, (coset && !inv) ? c.hi[0] : nullptr,
                        (coset && inv) ? c.lo[1] : nullptr, (coset && inv) ? c.hi[1] : nullptr, st);
 }
@@ -295,12 +285,12 @@ int lzk_ntt_prepare(uint32_t log_n)
 
 int lzk_ntt(lzk_fr_t* data, uint32_t log_n, int direction, void* stream)
 {
-    return run_ntt(reinterpret_cast<Fr*>(data), log_n, direction, 1, 0, as_stream(stream));
+    return ntt_run(reinterpret_cast<Fr*>(data), log_n, direction, 1, 0, nullptr, as_stream(stream));
 }
 
 int lzk_ntt_batch(lzk_fr_t* data, uint32_t log_n, uint32_t count, size_t stride, int direction, void* stream)
 {
-    return run_ntt(reinterpret_cast<Fr*>(data), log_n, direction, count, stride, as_stream(stream));
+    return ntt_run(reinterpret_cast<Fr*>(data), log_n, direction, count, stride, nullptr, as_stream(stream));
 }
 
 int lzk_number_theory_transformation(size_t deg, size_t log_deg, lzk_fr_t* coeffs, const lzk_fr_t* omega_powers,

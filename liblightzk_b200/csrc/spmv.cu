@@ -9,30 +9,9 @@
 // CSR with rows+1 offsets works unchanged.  Indices may be 32- or 64-bit
 // (the reference uses size_t).  Entries equal to one (Montgomery R mod r)
 // skip the product: z * 1 = z exactly.
-#include "common.cuh"
-#include "field.cuh"
+#include "r1cs.cuh"
 
 namespace lzk {
-
-struct CsrDev {
-    const Fr* val;
-    const void* col;
-    const void* rowp;
-    uint64_t rows, nnz;
-    uint32_t ib;  // index bytes
-};
-
-__device__ __forceinline__ uint64_t ld_index(const void* p, uint64_t i, uint32_t ib)
-{
-    return ib == 8 ? __ldg(reinterpret_cast<const unsigned long long*>(p) + i)
-                   : (uint64_t)__ldg(reinterpret_cast<const unsigned int*>(p) + i);
-}
-
-__device__ __forceinline__ bool is_mont_one(const Fr& v)
-{
-    Fr o = Fr::one();
-    return v == o;
-}
 
 __global__ void __launch_bounds__(256) k_spmv3(CsrDev m0, CsrDev m1, CsrDev m2, const Fr* __restrict__ z,
                                                 Fr* __restrict__ o0, Fr* __restrict__ o1, Fr* __restrict__ o2)
@@ -40,26 +19,7 @@ __global__ void __launch_bounds__(256) k_spmv3(CsrDev m0, CsrDev m1, CsrDev m2, 
     const CsrDev& M = blockIdx.y == 0 ? m0 : (blockIdx.y == 1 ? m1 : m2);
     Fr* out = blockIdx.y == 0 ? o0 : (blockIdx.y == 1 ? o1 : o2);
     if (!out) return;
-    for (uint64_t i = gtid(); i < M.rows; i += gstride()) {
-        uint64_t s = ld_index(M.rowp, i, M.ib);
-        uint64_t e = (i + 1 < M.rows) ? ld_index(M.rowp, i + 1, M.ib) : M.nnz;
-        Fr acc = Fr::zero();
-        for (uint64_t j = s; j < e; j++) {
-            Fr v = ldg_elem(M.val + j);
-            Fr x = ldg_elem(z + ld_index(M.col, j, M.ib));
-            acc = add(acc, is_mont_one(v) ? x : mul(x, v));
-        }
-        st_elem(out + i, acc);
-    }
-}
-
-static int to_dev(const lzk_csr* c, CsrDev& d)
-{
-    if (!c) { d = CsrDev{nullptr, nullptr, nullptr, 0, 0, 4}; return LZK_OK; }
-    if ((c->index_bytes != 4 && c->index_bytes != 8) || (c->rows && !c->row_ptr) || (c->nnz && (!c->val || !c->col_idx)))
-        return LZK_EINVAL;
-    d = CsrDev{reinterpret_cast<const Fr*>(c->val), c->col_idx, c->row_ptr, c->rows, c->nnz, c->index_bytes};
-    return LZK_OK;
+    for (uint64_t i = gtid(); i < M.rows; i += gstride()) st_elem(out + i, row_dot(M, i, z));
 }
 
 }  // namespace lzk
@@ -74,9 +34,9 @@ int lzk_spmv3(const lzk_csr* A, const lzk_csr* B, const lzk_csr* C, const lzk_fr
     if (!z && ((A && A->nnz) || (B && B->nnz) || (C && C->nnz))) return LZK_EINVAL;
     if ((A && !Az) || (B && !Bz) || (C && !Cz)) return LZK_EINVAL;
     CsrDev a, b, c;
-    LZK_TRY(to_dev(A, a));
-    LZK_TRY(to_dev(B, b));
-    LZK_TRY(to_dev(C, c));
+    LZK_TRY(csr_to_dev(A, a));
+    LZK_TRY(csr_to_dev(B, b));
+    LZK_TRY(csr_to_dev(C, c));
     uint64_t rows = a.rows > b.rows ? a.rows : b.rows;
     rows = rows > c.rows ? rows : c.rows;
     if (rows == 0) return LZK_OK;

@@ -1,0 +1,143 @@
+// trace.cu -- opt-in CUDA-event tracing of named device regions, and the
+// integer multiply-add throughput probe used as the roofline denominator.
+//
+// Tracing replaces the reference's wall-clock Timer + CUDA_DEBUG pairs
+// (timer.cu:3-16, device-utils.cuh:3), which synchronise the device after
+// every phase; here a traced region only records two events on its stream,
+// and durations are resolved when the host asks for them.
+#include "common.cuh"
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace lzk {
+
+struct TraceRec {
+    std::string name;
+    cudaEvent_t a, b;
+};
+
+static std::mutex g_tr_mu;
+static bool g_tr_on = false;
+static std::vector<TraceRec> g_tr_pending;
+static std::map<std::string, std::pair<double, uint64_t>> g_tr_sum;
+
+bool trace_on() { return g_tr_on; }
+
+void* trace_begin(const char* name, cudaStream_t st)
+{
+    if (!g_tr_on) return nullptr;
+    TraceRec* r = new TraceRec{name, nullptr, nullptr};
+    cudaEventCreate(&r->a);
+    cudaEventCreate(&r->b);
+    cudaEventRecord(r->a, st);
+    return r;
+}
+
+void trace_end(void* h, cudaStream_t st)
+{
+    if (!h) return;
+    TraceRec* r = static_cast<TraceRec*>(h);
+    cudaEventRecord(r->b, st);
+    std::lock_guard<std::mutex> g(g_tr_mu);
+    g_tr_pending.push_back(*r);
+    delete r;
+}
+
+static void resolve()
+{
+    for (auto& r : g_tr_pending) {
+        float ms = 0.f;
+        if (cudaEventSynchronize(r.b) == cudaSuccess && cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+            auto& s = g_tr_sum[r.name];
+            s.first += ms;
+            s.second += 1;
+        }
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    g_tr_pending.clear();
+    cudaGetLastError();
+}
+
+// Independent 32-bit multiply-add carry chains: each thread runs 8
+// interleaved chains of mad.lo.cc / madc.hi.cc, the instruction mix of the
+// Montgomery products.
+__global__ void k_imad_probe(uint32_t iters, uint32_t seed, uint32_t* sink)
+{
+    uint32_t x[8], y = seed ^ threadIdx.x, acc = 0;
+    for (int i = 0; i < 8; i++) x[i] = seed * (i + 3) + blockIdx.x;
+    for (uint32_t it = 0; it < iters; it++) {
+        #pragma unroll
+        for (int i = 0; i < 8; i++) {
+            asm volatile("mad.lo.cc.u32 %0, %0, %1, %0;\n\tmadc.hi.cc.u32 %0, %0, %1, %0;\n\t"
+                         "madc.lo.cc.u32 %0, %0, %1, %0;\n\tmadc.hi.u32 %0, %0, %1, %0;"
+                         : "+r"(x[i]) : "r"(y));
+        }
+    }
+    for (int i = 0; i < 8; i++) acc ^= x[i];
+    if (acc == 0x12345678u) sink[0] = acc;
+}
+
+}  // namespace lzk
+
+using namespace lzk;
+
+extern "C" {
+
+void lzk_trace_enable(int on)
+{
+    std::lock_guard<std::mutex> g(g_tr_mu);
+    g_tr_on = on != 0;
+}
+
+void lzk_trace_reset(void)
+{
+    std::lock_guard<std::mutex> g(g_tr_mu);
+    resolve();
+    g_tr_sum.clear();
+}
+
+int lzk_trace_get(const char* name, double* total_ms, uint64_t* count)
+{
+    if (!name || !total_ms || !count) return LZK_EINVAL;
+    std::lock_guard<std::mutex> g(g_tr_mu);
+    resolve();
+    auto it = g_tr_sum.find(name);
+    *total_ms = it == g_tr_sum.end() ? 0.0 : it->second.first;
+    *count = it == g_tr_sum.end() ? 0 : it->second.second;
+    return LZK_OK;
+}
+
+// Measured 32-bit integer multiply-add rate of this device (operations per
+// second, one mad.lo/madc.hi = one operation).  Synchronous; ~0.1 s.
+int lzk_probe_imad_rate(double* ops_per_s)
+{
+    if (!ops_per_s) return LZK_EINVAL;
+    int dev, sms;
+    LZK_CUDA(cudaGetDevice(&dev));
+    LZK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    uint32_t* sink;
+    LZK_CUDA(cudaMalloc(&sink, 4));
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const uint32_t iters = 4096, threads = 256, blocks = (uint32_t)sms * 8;
+    k_imad_probe<<<blocks, threads>>>(64, 1u, sink);  // warm-up
+    cudaEventRecord(a);
+    k_imad_probe<<<blocks, threads>>>(iters, 1u, sink);
+    cudaEventRecord(b);
+    cudaError_t e = cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(sink);
+    if (e != cudaSuccess) return cuda_status(e);
+    double ops = (double)blocks * threads * iters * 8.0 * 4.0;
+    *ops_per_s = ops / (ms * 1e-3);
+    return LZK_OK;
+}
+
+}  // extern "C"

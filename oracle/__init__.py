@@ -242,3 +242,65 @@ class Oracle(_Lib):
 
 def have_ref():
     return os.path.exists(REF_SO)
+
+
+class _OrcCsr(ctypes.Structure):
+    _fields_ = [("val", _P), ("col", _P), ("row_ptr", _P), ("rows", ctypes.c_size_t), ("nnz", ctypes.c_size_t)]
+
+
+class _OrcG16(ctypes.Structure):
+    _fields_ = [("A", _OrcCsr), ("B", _OrcCsr), ("C", _OrcCsr), ("n_vars", ctypes.c_size_t),
+                ("n_public", ctypes.c_size_t), ("log_m", ctypes.c_uint32),
+                ("a_query", _P), ("b1_query", _P), ("b2_query", _P), ("l_query", _P), ("h_query", _P),
+                ("alpha1", _P), ("beta1", _P), ("delta1", _P), ("beta2", _P), ("delta2", _P)]
+
+
+def _groth16_struct(mats, rows, n_vars, n_public, log_m, keys):
+    """mats: 3 tuples (val, col, row_ptr) of numpy arrays, row_ptr with
+    `rows` or rows+1 entries; keys: dict of affine numpy arrays."""
+    keep = []
+    g = _OrcG16()
+    for name, (val, col, rp) in zip("ABC", mats):
+        val, col, rp = _u64(val), _u64(col), _u64(rp)
+        keep += [val, col, rp]
+        setattr(g, name, _OrcCsr(_p(val), _p(col), _p(rp), rows, val.size // 4))
+    g.n_vars, g.n_public, g.log_m = n_vars, n_public, log_m
+    for k in ("a_query", "b1_query", "b2_query", "l_query", "h_query", "alpha1", "beta1", "delta1", "beta2",
+              "delta2"):
+        arr = _u64(keys[k])
+        keep.append(arr)
+        setattr(g, k, _p(arr))
+    return g, keep
+
+
+def _oracle_groth16(self, mats, rows, n_vars, n_public, log_m, keys, z, r, s, mode):
+    g, keep = _groth16_struct(mats, rows, n_vars, n_public, log_m, keys)
+    z, r, s = _u64(z), _u64(r), _u64(s)
+    pa = np.zeros((3, 4), np.uint64)
+    pb = np.zeros((3, 2, 4), np.uint64)
+    pc = np.zeros((3, 4), np.uint64)
+    rc = self.lib.orc_groth16_prove(ctypes.byref(g), ctypes.c_int(mode), _p(z), _p(r), _p(s), _p(pa), _p(pb), _p(pc))
+    assert rc == 0
+    return pa, pb, pc
+
+
+def _oracle_groth16_h(self, mats, rows, n_vars, n_public, log_m, z, mode):
+    dummy = {k: np.zeros(8, np.uint64) for k in ("a_query", "b1_query", "b2_query", "l_query", "h_query", "alpha1",
+                                                  "beta1", "delta1", "beta2", "delta2")}
+    g, keep = _groth16_struct(mats, rows, n_vars, n_public, log_m, dummy)
+    h = np.zeros(((1 << log_m) - 1, 4), np.uint64)
+    assert self.lib.orc_groth16_h(ctypes.byref(g), ctypes.c_int(mode), _p(_u64(z)), _p(h)) == 0
+    return h
+
+
+def _oracle_assemble(self, alpha1, beta1, delta1, beta2, delta2, g1res, g2res, r, s):
+    og1 = np.zeros((2, 3, 4), np.uint64)
+    og2 = np.zeros((3, 2, 4), np.uint64)
+    args = [_u64(x) for x in (alpha1, beta1, delta1, beta2, delta2, g1res, g2res, r, s)]
+    self.lib.orc_groth16_assemble(*[_p(a) for a in args], _p(og1), _p(og2))
+    return og1, og2
+
+
+Oracle.groth16_prove = _oracle_groth16
+Oracle.groth16_h = _oracle_groth16_h
+Oracle.groth16_assemble = _oracle_assemble

@@ -539,3 +539,106 @@ void orc_spmv(const uint64_t* val, const uint64_t* col_idx, const uint64_t* row_
         memcpy(out + 4 * i, acc.l, 32);
     }
 }
+
+/* ---------------- Groth16 ---------------- */
+
+static void jac_from_aff_g1(g1j* o, const uint64_t* aff) { g1_from_aff(o, (const fe*)aff); }
+static void jac_from_aff_g2(g2j* o, const uint64_t* aff) { g2_from_aff(o, (const fe2*)aff); }
+
+static void fr_canon(const uint64_t* m, uint64_t* c) { f_from_mont(&FRD, (fe*)c, (const fe*)m); }
+
+/* groth16.cuh:211-215 */
+void orc_groth16_assemble(const uint64_t* alpha1, const uint64_t* beta1, const uint64_t* delta1,
+                          const uint64_t* beta2, const uint64_t* delta2,
+                          const uint64_t* g1res, const uint64_t* g2res,
+                          const uint64_t* r, const uint64_t* s, uint64_t* out_g1, uint64_t* out_g2)
+{
+    const g1j *a1 = (const g1j*)alpha1, *b1 = (const g1j*)beta1, *d1 = (const g1j*)delta1;
+    const g2j *b2 = (const g2j*)beta2, *d2 = (const g2j*)delta2;
+    const g1j* res = (const g1j*)g1res;
+    uint64_t rc[4], sc[4], nrsc[4];
+    fe nr, nrs;
+    fr_canon(r, rc); fr_canon(s, sc);
+    f_neg(&FRD, &nr, (const fe*)r); f_mul(&FRD, &nrs, &nr, (const fe*)s);
+    fr_canon(nrs.l, nrsc);
+    g1j t, Ar, Bs1, Krs;
+    g1_add(&Ar, a1, &res[0]); g1_mul(&t, d1, rc); g1_add(&Ar, &Ar, &t);
+    g1_add(&Bs1, b1, &res[1]); g1_mul(&t, d1, sc); g1_add(&Bs1, &Bs1, &t);
+    g1_mul(&Krs, &Ar, sc);
+    g1_mul(&t, &Bs1, rc); g1_add(&Krs, &Krs, &t);
+    g1_mul(&t, d1, nrsc); g1_add(&Krs, &Krs, &t);
+    g1_add(&Krs, &Krs, &res[2]);
+    g1_add(&t, &Krs, &res[3]);
+    memcpy(out_g1, &Ar, 96); memcpy(out_g1 + 12, &t, 96);
+    g2j u, Bs2;
+    g2_add(&Bs2, b2, (const g2j*)g2res); g2_mul(&u, d2, sc); g2_add(&Bs2, &Bs2, &u);
+    memcpy(out_g2, &Bs2, 192);
+}
+
+static void csr_spmv(const orc_csr* m, const uint64_t* z, uint64_t* out)
+{
+    orc_spmv(m->val, m->col, m->row_ptr, m->rows, m->nnz, z, out);
+}
+
+int orc_groth16_h(const orc_groth16* g, int mode, const uint64_t* z, uint64_t* h_out)
+{
+    size_t M = (size_t)1 << g->log_m;
+    if (g->A.rows > M || g->B.rows > M || g->C.rows > M || g->log_m < 1 || g->log_m > 26) return -1;
+    size_t L = mode == 1 ? 2 * M : M;
+    fe* x[3];
+    for (int q = 0; q < 3; q++) { x[q] = (fe*)calloc(L, sizeof(fe)); }
+    csr_spmv(&g->A, z, (uint64_t*)x[0]);
+    csr_spmv(&g->B, z, (uint64_t*)x[1]);
+    csr_spmv(&g->C, z, (uint64_t*)x[2]);
+    if (mode == 1) {
+        for (int q = 0; q < 3; q++) orc_ntt((uint64_t*)x[q], g->log_m, 1);          /* iNTT_M, * M^-1 */
+        for (int q = 0; q < 3; q++) orc_ntt((uint64_t*)x[q], g->log_m + 1, 0);      /* NTT_2M */
+        for (size_t j = 0; j < L; j++) { fe t; f_mul(&FRD, &t, &x[0][j], &x[1][j]); f_sub(&FRD, &x[0][j], &t, &x[2][j]); }
+        /* iNTT_2M with the (4M)^-1 entry of ntt_setup (groth16-operator.cuh:13) */
+        fe w; orc_ntt_table(1, g->log_m + 1, w.l);
+        fe* pw = (fe*)malloc(sizeof(fe) * M);
+        f_one(&FRD, &pw[0]);
+        for (size_t i = 1; i < M; i++) f_mul(&FRD, &pw[i], &pw[i - 1], &w);
+        fe sc; orc_ntt_table(2, g->log_m + 2, sc.l);
+        orc_ntt_ref((uint64_t*)x[0], L, (const uint64_t*)pw, sc.l);
+        free(pw);
+        memcpy(h_out, &x[0][M + 1], sizeof(fe) * (M - 1));
+    } else {
+        for (int q = 0; q < 3; q++) { orc_ntt((uint64_t*)x[q], g->log_m, 1); orc_ntt((uint64_t*)x[q], g->log_m, 2); }
+        /* Z(g w^j) = g^M - 1 for every j */
+        fe gm, one, zinv; fq_zero(&gm); gm.l[0] = 5; f_to_mont(&FRD, &gm, &gm);
+        for (uint32_t i = 0; i < g->log_m; i++) f_mul(&FRD, &gm, &gm, &gm);
+        f_one(&FRD, &one); f_sub(&FRD, &gm, &gm, &one); f_inv(&FRD, &zinv, &gm);
+        for (size_t j = 0; j < M; j++) {
+            fe t; f_mul(&FRD, &t, &x[0][j], &x[1][j]); f_sub(&FRD, &t, &t, &x[2][j]); f_mul(&FRD, &x[0][j], &t, &zinv);
+        }
+        orc_ntt((uint64_t*)x[0], g->log_m, 3);
+        memcpy(h_out, &x[0][0], sizeof(fe) * (M - 1));
+    }
+    for (int q = 0; q < 3; q++) free(x[q]);
+    return 0;
+}
+
+int orc_groth16_prove(const orc_groth16* g, int mode, const uint64_t* z, const uint64_t* r, const uint64_t* s,
+                      uint64_t* proof_a, uint64_t* proof_b, uint64_t* proof_c)
+{
+    size_t M = (size_t)1 << g->log_m;
+    uint64_t* h = (uint64_t*)malloc(32 * M);
+    if (orc_groth16_h(g, mode, z, h)) { free(h); return -1; }
+    uint64_t g1res[4 * 12], g2res[24];
+    size_t nl = g->n_vars - g->n_public - 1;
+    orc_g1_msm(z, g->a_query, g->n_vars, g1res);
+    orc_g1_msm(z, g->b1_query, g->n_vars, g1res + 12);
+    orc_g1_msm(z + 4 * (g->n_public + 1), g->l_query, nl, g1res + 24);
+    orc_g1_msm(h, g->h_query, M - 1, g1res + 36);
+    orc_g2_msm(z, g->b2_query, g->n_vars, g2res);
+    free(h);
+    g1j a1, b1, d1; g2j b2, d2;
+    jac_from_aff_g1(&a1, g->alpha1); jac_from_aff_g1(&b1, g->beta1); jac_from_aff_g1(&d1, g->delta1);
+    jac_from_aff_g2(&b2, g->beta2); jac_from_aff_g2(&d2, g->delta2);
+    uint64_t og1[24], og2[24];
+    orc_groth16_assemble((uint64_t*)&a1, (uint64_t*)&b1, (uint64_t*)&d1, (uint64_t*)&b2, (uint64_t*)&d2,
+                         g1res, g2res, r, s, og1, og2);
+    memcpy(proof_a, og1, 96); memcpy(proof_c, og1 + 12, 96); memcpy(proof_b, og2, 192);
+    return 0;
+}

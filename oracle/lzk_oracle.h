@@ -84,3 +84,47 @@ void orc_spmv(const uint64_t* val, const uint64_t* col_idx, const uint64_t* row_
 #ifdef __cplusplus
 }
 #endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------- Groth16 (include/protocol/groth16.cuh) ---------------- */
+typedef struct {
+    const uint64_t *val, *col, *row_ptr;  /* row_ptr: rows entries; last row ends at nnz */
+    size_t rows, nnz;
+} orc_csr;
+
+typedef struct {
+    orc_csr A, B, C;           /* constraints = rows <= 2^log_m */
+    size_t n_vars;             /* N + 1, z[0] = 1 */
+    size_t n_public;           /* k (reference) / l: L query covers z[k+1 .. N] */
+    uint32_t log_m;            /* evaluation domain M = 2^log_m */
+    /* affine keys (x, y); G1 8 limbs, G2 16 limbs per point */
+    const uint64_t *a_query, *b1_query, *b2_query, *l_query, *h_query;
+    const uint64_t *alpha1, *beta1, *delta1, *beta2, *delta2;
+} orc_groth16;
+
+/* Phase 6 of Groth16::Prove (groth16.cuh:209-215) from the five MSM
+ * results (Jacobian): out_g1 = [Ar, Krs + HZ], out_g2 = [Bs2]. */
+void orc_groth16_assemble(const uint64_t* alpha1, const uint64_t* beta1, const uint64_t* delta1,
+                          const uint64_t* beta2, const uint64_t* delta2,
+                          const uint64_t* g1res, const uint64_t* g2res,
+                          const uint64_t* r, const uint64_t* s, uint64_t* out_g1, uint64_t* out_g2);
+
+/* H-polynomial scalars (M - 1 of them).
+ * mode 1 = the reference chain (groth16.cuh:159-185): iNTT_M (scale M^-1),
+ *   NTT_2M of the zero-padded coefficients, A*B - C, iNTT_2M with the
+ *   table's (4M)^-1 scale; scalars = coefficients M+1 .. 2M-1 (198).
+ * mode 0 = standard quotient on the coset g<w_M>, g = 5: iNTT_M, coset NTT,
+ *   (A*B - C) / (g^M - 1), coset iNTT; scalars = h_0 .. h_{M-2}. */
+int orc_groth16_h(const orc_groth16* g, int mode, const uint64_t* z, uint64_t* h_out);
+
+/* Full prove: SpMV, H scalars, the five MSMs, Phase 6.  Outputs Jacobian
+ * proof A (G1), B (G2), C (G1). */
+int orc_groth16_prove(const orc_groth16* g, int mode, const uint64_t* z, const uint64_t* r, const uint64_t* s,
+                      uint64_t* proof_a, uint64_t* proof_b, uint64_t* proof_c);
+
+#ifdef __cplusplus
+}
+#endif
