@@ -11,6 +11,7 @@ struct G2 { using F = Fq2; };
 
 constexpr uint32_t kAccChunk = 32;   // sorted entries per accumulation thread
 constexpr uint32_t kLevelL = 8;      // buckets per thread in a reduction level
+constexpr uint32_t kFixSmall = 8;    // partials a single fix-up thread folds
 
 struct MsmPlan {
     size_t n = 0;
@@ -24,7 +25,7 @@ struct MsmPlan {
     size_t max_entries = 0;
     size_t chunks = 0;
     // workspace offsets
-    size_t o_cnt, o_off, o_ent, o_bsum, o_head, o_tail, o_lr0, o_la0, o_lr1, o_la1, bytes;
+    size_t o_cnt, o_off, o_ent, o_bsum, o_head, o_tail, o_lr0, o_la0, o_lr1, o_la1, o_scan, o_large, bytes;
 };
 
 inline uint32_t windows_for(uint32_t c) { return (255 + c - 1) / c; }
@@ -51,12 +52,15 @@ inline void plan_msm(MsmPlan& p, size_t n, uint32_t c, bool shared, size_t strid
     p.o_la0 = cv.take<X>(lvl);
     p.o_lr1 = cv.take<X>(lvl);
     p.o_la1 = cv.take<X>(lvl);
+    p.o_scan = cv.take<uint32_t>((p.B + 4095) / 4096 + 1);
+    p.o_large = cv.take<uint32_t>(p.chunks / 8 + 2);   // count, then bucket ids
     p.bytes = cv.off;
 }
 
 // counting sort of the signed digits of all scalars into bucket lists:
 // cnt/off/ent as carved by plan_msm (msm_sort.cu)
-int msm_sort(const MsmPlan& p, const Fr* scalars, uint32_t* cnt, uint32_t* off, uint32_t* ent, cudaStream_t st);
+int msm_sort(const MsmPlan& p, const Fr* scalars, uint32_t* cnt, uint32_t* off, uint32_t* ent, uint32_t* bsums,
+             cudaStream_t st);
 uint32_t msm_autotune(int group, size_t n, bool shared);
 
 // largest b in [lo, B) with off[b] <= e
@@ -111,16 +115,48 @@ __global__ void __launch_bounds__(256) k_accumulate(const Aff<F>* __restrict__ b
 
 template <class F>
 __global__ void k_fixup(const uint32_t* __restrict__ off, uint32_t B, XYZZ<F>* __restrict__ bsum,
-                        const XYZZ<F>* __restrict__ head, const XYZZ<F>* __restrict__ tail)
+                        const XYZZ<F>* __restrict__ head, const XYZZ<F>* __restrict__ tail, uint32_t* __restrict__ large)
 {
     for (uint64_t b = gtid(); b < B; b += gstride()) {
         uint32_t s = off[b], e = off[b + 1];
         if (s == e) continue;
         uint32_t c0 = s / kAccChunk, c1 = (e - 1) / kAccChunk;
         if (c0 == c1) continue;
+        if (c1 - c0 > kFixSmall) {
+            large[1 + atomicAdd(large, 1u)] = (uint32_t)b;
+            continue;
+        }
         XYZZ<F> acc = ld_elem(tail + c0);
         for (uint32_t c = c0 + 1; c <= c1; c++) acc = xyzz_add_cold(acc, ld_elem(head + c));
         st_elem(bsum + b, acc);
+    }
+}
+
+// One block per listed bucket: strided partial sums, then a tree in shared
+// memory.  Partial q of bucket b is tail[c0] (q = 0) or head[c0 + q].
+template <class F>
+__global__ void k_fixup_large(const uint32_t* __restrict__ off, XYZZ<F>* __restrict__ bsum,
+                              const XYZZ<F>* __restrict__ head, const XYZZ<F>* __restrict__ tail,
+                              const uint32_t* __restrict__ large)
+{
+    extern __shared__ uint4 fx_raw[];
+    XYZZ<F>* sm = reinterpret_cast<XYZZ<F>*>(fx_raw);
+    uint32_t nl = large[0];
+    for (uint32_t idx = blockIdx.x; idx < nl; idx += gridDim.x) {
+        uint32_t b = large[1 + idx];
+        uint32_t c0 = off[b] / kAccChunk, c1 = (off[b + 1] - 1) / kAccChunk;
+        uint32_t np = c1 - c0 + 1;
+        XYZZ<F> acc = xyzz_inf<F>();
+        for (uint32_t q = threadIdx.x; q < np; q += blockDim.x)
+            acc = xyzz_add_cold(acc, ld_elem(q ? head + c0 + q : tail + c0));
+        st_elem(sm + threadIdx.x, acc);
+        __syncthreads();
+        for (uint32_t h = blockDim.x / 2; h > 0; h >>= 1) {
+            if (threadIdx.x < h) st_elem(sm + threadIdx.x, xyzz_add_cold(ld_elem(sm + threadIdx.x), ld_elem(sm + threadIdx.x + h)));
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) st_elem(bsum + b, ld_elem(sm));
+        __syncthreads();
     }
 }
 
@@ -209,11 +245,18 @@ int run_msm(const Fr* scalars, const Aff<typename Gp::F>* bases, size_t n, Jac<t
     X* lr[2] = {reinterpret_cast<X*>(base + p.o_lr0), reinterpret_cast<X*>(base + p.o_lr1)};
     X* la[2] = {reinterpret_cast<X*>(base + p.o_la0), reinterpret_cast<X*>(base + p.o_la1)};
 
-    LZK_TRY(msm_sort(p, scalars, cnt, off, ent, st));
+    uint32_t* bsums = reinterpret_cast<uint32_t*>(base + p.o_scan);
+    uint32_t* large = reinterpret_cast<uint32_t*>(base + p.o_large);
+    LZK_TRY(msm_sort(p, scalars, cnt, off, ent, bsums, st));
     void* tr = trace_begin(sizeof(F) == 32 ? "msm_g1_accumulate" : "msm_g2_accumulate", st);
     k_accumulate<F><<<grid_for(p.chunks, 256), 256, 0, st>>>(bases, ent, off, p.B, p.chunks, bsum, head, tail);
     trace_end(tr, st);
-    k_fixup<F><<<grid_for(p.B, 256, 148 * 8), 256, 0, st>>>(off, p.B, bsum, head, tail);
+    LZK_CUDA(cudaMemsetAsync(large, 0, sizeof(uint32_t), st));
+    k_fixup<F><<<grid_for(p.B, 256, 148 * 8), 256, 0, st>>>(off, p.B, bsum, head, tail, large);
+    {
+        constexpr unsigned fx_threads = 32768 / sizeof(X);   // 32 KB of shared memory
+        k_fixup_large<F><<<148 * 2, fx_threads, fx_threads * sizeof(X), st>>>(off, bsum, head, tail, large);
+    }
     LZK_TRY(launch_status());
 
     // weighted sums per bucket set

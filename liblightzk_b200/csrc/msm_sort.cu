@@ -5,13 +5,18 @@
 // Pipeline per call, all on one stream, no host synchronisation:
 //   1. k_count     signed c-bit digits of every scalar; a histogram of
 //                  (window, |digit|) buckets (global atomics).
-//   2. k_scan      exclusive prefix sum -> bucket offsets; off[B] = entries.
+//   2. k_scan_*    exclusive prefix sum -> bucket offsets; off[B] = entries.
 //   3. k_scatter   counting-sort scatter of (point index, sign) entries.
 //   4. k_accumulate each thread adds exactly K consecutive sorted entries
 //                  (XYZZ mixed adds of affine bases), so the work is even
 //                  whatever the bucket sizes; segments that cross a chunk
 //                  boundary leave partial sums.
-//   5. k_fixup     folds those partial sums into their buckets.
+//   5. k_fixup     folds those partial sums into their buckets: one thread
+//                  per bucket with at most kFixSmall partials, one block and
+//                  a shared-memory tree per larger bucket (k_fixup_large),
+//                  so a bucket holding most of the entries (all scalars
+//                  equal, or the sparse top window of 254-bit scalars at
+//                  some widths) is summed with logarithmic depth.
 //   6. k_level     weighted bucket sums  sum_j j*B_j  by segmented running
 //                  sums, L buckets per thread, repeated until one value
 //                  per window is left.
@@ -88,37 +93,76 @@ __global__ void k_scatter(const Fr* __restrict__ scalars, size_t n, uint32_t c, 
     }
 }
 
-// Exclusive scan of cnt[0..B) into off[0..B], off[B] = total.  One block of
-// 1024 threads; thread t owns a contiguous run of ceil(B/1024) counters.
-__global__ void __launch_bounds__(1024) k_scan(const uint32_t* __restrict__ cnt, uint32_t B, uint32_t* __restrict__ off)
+// Exclusive scan of cnt[0..B) into off[0..B], off[B] = total, in three
+// passes: per-block scans of 4096 counters (1024 threads x 4), a scan of the
+// block totals in one block, and the add-back of each block's offset.
+constexpr uint32_t kScanBlock = 4096;
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t* warp_tot, uint32_t& total)
 {
-    __shared__ uint32_t warp_tot[32];
-    uint32_t per = (B + 1023) / 1024;
-    uint32_t beg = threadIdx.x * per, end = min(beg + per, B);
-    uint32_t sum = 0;
-    for (uint32_t i = beg; i < end; i++) sum += cnt[i];
-    uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    uint32_t x = sum;
-    for (int o = 1; o < 32; o <<= 1) { uint32_t y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= (uint32_t)o) x += y; }
-    if (lane == 31) warp_tot[wid] = x;
+    uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t v = x;
+    for (int o = 1; o < 32; o <<= 1) { uint32_t y = __shfl_up_sync(0xffffffffu, v, o); if (lane >= (uint32_t)o) v += y; }
+    if (lane == 31) warp_tot[wid] = v;
     __syncthreads();
     if (wid == 0) {
-        uint32_t t = warp_tot[lane];
+        uint32_t t = lane < nw ? warp_tot[lane] : 0u;
         for (int o = 1; o < 32; o <<= 1) { uint32_t y = __shfl_up_sync(0xffffffffu, t, o); if (lane >= (uint32_t)o) t += y; }
         warp_tot[lane] = t;
     }
     __syncthreads();
-    uint32_t run = x - sum + (wid ? warp_tot[wid - 1] : 0u);
-    for (uint32_t i = beg; i < end; i++) { off[i] = run; run += cnt[i]; }
-    if (threadIdx.x == 1023) off[B] = warp_tot[31];
+    total = warp_tot[nw - 1];
+    uint32_t r = v - x + (wid ? warp_tot[wid - 1] : 0u);
+    __syncthreads();
+    return r;
 }
 
-int msm_sort(const MsmPlan& p, const Fr* scalars, uint32_t* cnt, uint32_t* off, uint32_t* ent, cudaStream_t st)
+__global__ void __launch_bounds__(1024) k_scan_local(const uint32_t* __restrict__ cnt, uint32_t B,
+                                                     uint32_t* __restrict__ off, uint32_t* __restrict__ bsums)
+{
+    __shared__ uint32_t warp_tot[32];
+    uint32_t base = blockIdx.x * kScanBlock + threadIdx.x * 4;
+    uint32_t v[4];
+    for (int i = 0; i < 4; i++) v[i] = (base + i < B) ? cnt[base + i] : 0u;
+    uint32_t sum = v[0] + v[1] + v[2] + v[3], total;
+    uint32_t run = block_exclusive_scan(sum, warp_tot, total);
+    for (int i = 0; i < 4; i++) {
+        if (base + i < B) off[base + i] = run;
+        run += v[i];
+    }
+    if (threadIdx.x == 0) bsums[blockIdx.x] = total;
+}
+
+// in-place exclusive scan of nb block totals; off[B] = grand total
+__global__ void __launch_bounds__(1024) k_scan_top(uint32_t* __restrict__ bsums, uint32_t nb, uint32_t* __restrict__ off,
+                                                   uint32_t B)
+{
+    __shared__ uint32_t warp_tot[32];
+    uint32_t per = (nb + blockDim.x - 1) / blockDim.x;
+    uint32_t beg = threadIdx.x * per, end = min(beg + per, nb);
+    uint32_t sum = 0;
+    for (uint32_t i = beg; i < end; i++) sum += bsums[i];
+    uint32_t total;
+    uint32_t run = block_exclusive_scan(sum, warp_tot, total);
+    for (uint32_t i = beg; i < end; i++) { uint32_t t = bsums[i]; bsums[i] = run; run += t; }
+    if (threadIdx.x == 0) off[B] = total;
+}
+
+__global__ void k_scan_add(uint32_t* __restrict__ off, uint32_t B, const uint32_t* __restrict__ bsums)
+{
+    for (uint64_t i = gtid(); i < B; i += gstride()) off[i] += bsums[i / kScanBlock];
+}
+
+int msm_sort(const MsmPlan& p, const Fr* scalars, uint32_t* cnt, uint32_t* off, uint32_t* ent, uint32_t* bsums,
+             cudaStream_t st)
 {
     LZK_CUDA(cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * p.B, st));
     unsigned g = grid_for(p.n, 256, 148 * 16);
     k_count<<<g, 256, 0, st>>>(scalars, p.n, p.c, p.W, p.nb, p.shared, cnt);
-    k_scan<<<1, 1024, 0, st>>>(cnt, p.B, off);
+    uint32_t nblk = (p.B + kScanBlock - 1) / kScanBlock;
+    k_scan_local<<<nblk, 1024, 0, st>>>(cnt, p.B, off, bsums);
+    k_scan_top<<<1, 1024, 0, st>>>(bsums, nblk, off, p.B);
+    k_scan_add<<<grid_for(p.B, 256, 148 * 8), 256, 0, st>>>(off, p.B, bsums);
     k_scatter<<<g, 256, 0, st>>>(scalars, p.n, p.c, p.W, p.nb, p.shared, p.stride, off, cnt, ent);
     return launch_status();
 }
