@@ -43,6 +43,10 @@ def parse():
     ap.add_argument("--mode", choices=["standard", "reference"], default="standard")
     ap.add_argument("--window", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--case", choices=["prove", "msm-g1", "msm-g2", "ntt"], default="prove",
+                    help="prove = the benchmark; the others run one operator at --log-n for profiling")
+    ap.add_argument("--log-n", type=int, default=20)
+    ap.add_argument("--reps", type=int, default=3)
     return ap.parse_args()
 
 
@@ -176,6 +180,35 @@ def run_reference_arm(args, rank, world):
 
 
 # --------------------------------------------------------------- GPU side
+def run_case(args):
+    """one operator at 2^log_n, `reps` times, for profiling (prints ms)"""
+    import torch
+
+    from liblightzk_b200 import msm, ntt, synth
+    n = 1 << args.log_n
+    sc = synth.random_fr(n, 5, 77)
+    out = []
+    if args.case in ("msm-g1", "msm-g2"):
+        g = 1 if args.case == "msm-g1" else 2
+        bases = synth.fixed_base(g, synth.random_fr(n, 5, 78))
+        c = args.window
+        W = msm.windows_for(c)
+        table = msm.precompute(g, bases, c, W, n)
+        ws = torch.empty(msm.workspace_bytes(g, n, c, True, n), dtype=torch.uint8, device="cuda")
+        fn = lambda: msm.msm_precomputed(g, sc, table, c, W, n, workspace=ws)  # noqa: E731
+    else:
+        ntt.prepare(args.log_n)
+        fn = lambda: ntt.ntt(sc, args.log_n, ntt.COSET_FORWARD)  # noqa: E731
+    for _ in range(args.reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        out.append(a.elapsed_time(b))
+    print(json.dumps({"case": args.case, "log_n": args.log_n, "window": args.window, "ms": out}), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -183,6 +216,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
+        return
+    if args.case != "prove":
+        run_case(args)
         return
 
     import torch
@@ -228,6 +264,7 @@ def main():
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
+    launches0 = _capi.launch_count()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
@@ -237,6 +274,7 @@ def main():
         ev[k][1].record()
     e1.record()
     torch.cuda.synchronize()
+    launches = _capi.launch_count() - launches0
     _capi.trace_enable(False)
     ms_total = e0.elapsed_time(e1)
     lat = sorted(a.elapsed_time(b) for a, b in ev)
@@ -338,7 +376,7 @@ def main():
         "g1_msm_2e20_ms": g1_ms, "g1_msm_2e20_plain_ms": g1_plain_ms,
         "e2e": {"value": world * args.steps / (e2e_ms * 1e-3), "unit": "proofs/s",
                 "h2d_bytes_per_step": int(wits[0].numel() * 8), "d2h_bytes_per_step": groth16.PROOF_WORDS * 8},
-        "gpu_launches": None,
+        "gpu_launches": launches,
         "roofline": {"kernel": "k_accumulate<Fq> (G1 bucket accumulation)", "bound": "int",
                      "achieved": achieved / 1e12 if achieved else None, "peak": imad_peak / 1e12,
                      "unit": "T IMAD/s", "frac": (achieved / imad_peak) if achieved else None,

@@ -240,6 +240,8 @@ void lzk_trace_reset(void);
 /* Total device milliseconds and count of completed regions named `name`
  * since the last reset (waits for pending regions). */
 int lzk_trace_get(const char* name, double* total_ms, uint64_t* count);
+/* Number of kernels this library has launched so far (all devices). */
+uint64_t lzk_launch_count(void);
 /* Measured 32-bit integer multiply-add rate of the current device
  * (mad.lo/madc.hi operations per second); synchronous. */
 int lzk_probe_imad_rate(double* ops_per_s);

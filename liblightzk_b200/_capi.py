@@ -46,6 +46,7 @@ SIGNATURES = {
     "lzk_trace_reset": (None, []),
     "lzk_trace_get": (c_i, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64)]),
     "lzk_probe_imad_rate": (c_i, [ctypes.POINTER(ctypes.c_double)]),
+    "lzk_launch_count": (ctypes.c_uint64, []),
 }
 
 
@@ -137,3 +138,7 @@ def probe_imad_rate():
     r = ctypes.c_double()
     call("lzk_probe_imad_rate", ctypes.byref(r))
     return r.value
+
+
+def launch_count():
+    return int(lib().lzk_launch_count())

@@ -35,6 +35,10 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 
 inline size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
 
+// Count of kernel launches this library has enqueued (trace.cu); every
+// launch site is followed by note_launch().
+void note_launch();
+
 // Opt-in event tracing of named device regions (trace.cu): a no-op returning
 // nullptr unless lzk_trace_enable(1) was called.
 bool trace_on();

@@ -51,6 +51,22 @@ static __device__ __noinline__ Fq2 inverse(const Fq2& a)
     return {mul(a.c0, t), neg(mul(a.c1, t))};
 }
 
+// Products used by the point formulas: out-of-line Fq products (mul_call),
+// Fq2 products built from them.
+__device__ __forceinline__ Fq cmul(const Fq& a, const Fq& b) { return mul_call(a, b); }
+__device__ __forceinline__ Fq csqr(const Fq& a) { return mul_call(a, a); }
+__device__ __forceinline__ Fq2 cmul(const Fq2& a, const Fq2& b)
+{
+    Fq aa = mul_call(a.c0, b.c0), bb = mul_call(a.c1, b.c1);
+    Fq s = mul_call(add(a.c0, a.c1), add(b.c0, b.c1));
+    return {sub(aa, bb), sub(sub(s, aa), bb)};
+}
+__device__ __forceinline__ Fq2 csqr(const Fq2& a)
+{
+    Fq ab = mul_call(a.c0, a.c1);
+    return {mul_call(add(a.c0, a.c1), sub(a.c0, a.c1)), dbl(ab)};
+}
+
 // ---------------- point forms ----------------
 template <class F> struct Aff { F x, y; };
 template <class F> struct XYZZ { F X, Y, ZZ, ZZZ; };
@@ -70,13 +86,13 @@ template <class F> __device__ __forceinline__ XYZZ<F> xyzz_from_aff(const Aff<F>
 template <class F> __device__ __forceinline__ XYZZ<F> xyzz_mdbl(const Aff<F>& a)
 {
     F U = dbl(a.y);
-    F V = sqr(U);
-    F W = mul(U, V);
-    F S = mul(a.x, V);
-    F x2 = sqr(a.x);
+    F V = csqr(U);
+    F W = cmul(U, V);
+    F S = cmul(a.x, V);
+    F x2 = csqr(a.x);
     F M = add(dbl(x2), x2);
-    F X3 = sub(sqr(M), dbl(S));
-    F Y3 = sub(mul(M, sub(S, X3)), mul(W, a.y));
+    F X3 = sub(csqr(M), dbl(S));
+    F Y3 = sub(cmul(M, sub(S, X3)), cmul(W, a.y));
     return {X3, Y3, V, W};
 }
 
@@ -85,14 +101,14 @@ template <class F> __device__ __forceinline__ XYZZ<F> xyzz_dbl(const XYZZ<F>& p)
 {
     if (xyzz_is_inf(p)) return p;
     F U = dbl(p.Y);
-    F V = sqr(U);
-    F W = mul(U, V);
-    F S = mul(p.X, V);
-    F x2 = sqr(p.X);
+    F V = csqr(U);
+    F W = cmul(U, V);
+    F S = cmul(p.X, V);
+    F x2 = csqr(p.X);
     F M = add(dbl(x2), x2);
-    F X3 = sub(sqr(M), dbl(S));
-    F Y3 = sub(mul(M, sub(S, X3)), mul(W, p.Y));
-    return {X3, Y3, mul(V, p.ZZ), mul(W, p.ZZZ)};
+    F X3 = sub(csqr(M), dbl(S));
+    F Y3 = sub(cmul(M, sub(S, X3)), cmul(W, p.Y));
+    return {X3, Y3, cmul(V, p.ZZ), cmul(W, p.ZZZ)};
 }
 
 // P + Q with Q affine (madd-2008-s); handles infinity, P == Q and P == -Q
@@ -100,20 +116,20 @@ template <class F> __device__ __forceinline__ XYZZ<F> xyzz_madd(const XYZZ<F>& p
 {
     if (aff_is_inf(q)) return p;
     if (xyzz_is_inf(p)) return xyzz_from_aff(q);
-    F U2 = mul(q.x, p.ZZ);
-    F S2 = mul(q.y, p.ZZZ);
+    F U2 = cmul(q.x, p.ZZ);
+    F S2 = cmul(q.y, p.ZZZ);
     F P = sub(U2, p.X);
     F R = sub(S2, p.Y);
     if (P.is_zero()) {
         if (R.is_zero()) return xyzz_mdbl(q);
         return xyzz_inf<F>();
     }
-    F PP = sqr(P);
-    F PPP = mul(P, PP);
-    F Q = mul(p.X, PP);
-    F X3 = sub(sub(sqr(R), PPP), dbl(Q));
-    F Y3 = sub(mul(R, sub(Q, X3)), mul(p.Y, PPP));
-    return {X3, Y3, mul(p.ZZ, PP), mul(p.ZZZ, PPP)};
+    F PP = csqr(P);
+    F PPP = cmul(P, PP);
+    F Q = cmul(p.X, PP);
+    F X3 = sub(sub(csqr(R), PPP), dbl(Q));
+    F Y3 = sub(cmul(R, sub(Q, X3)), cmul(p.Y, PPP));
+    return {X3, Y3, cmul(p.ZZ, PP), cmul(p.ZZZ, PPP)};
 }
 
 // P + Q (add-2008-s)
@@ -121,22 +137,22 @@ template <class F> __device__ __forceinline__ XYZZ<F> xyzz_add(const XYZZ<F>& p,
 {
     if (xyzz_is_inf(q)) return p;
     if (xyzz_is_inf(p)) return q;
-    F U1 = mul(p.X, q.ZZ);
-    F U2 = mul(q.X, p.ZZ);
-    F S1 = mul(p.Y, q.ZZZ);
-    F S2 = mul(q.Y, p.ZZZ);
+    F U1 = cmul(p.X, q.ZZ);
+    F U2 = cmul(q.X, p.ZZ);
+    F S1 = cmul(p.Y, q.ZZZ);
+    F S2 = cmul(q.Y, p.ZZZ);
     F P = sub(U2, U1);
     F R = sub(S2, S1);
     if (P.is_zero()) {
         if (R.is_zero()) return xyzz_dbl(p);
         return xyzz_inf<F>();
     }
-    F PP = sqr(P);
-    F PPP = mul(P, PP);
-    F Q = mul(U1, PP);
-    F X3 = sub(sub(sqr(R), PPP), dbl(Q));
-    F Y3 = sub(mul(R, sub(Q, X3)), mul(S1, PPP));
-    return {X3, Y3, mul(mul(p.ZZ, q.ZZ), PP), mul(mul(p.ZZZ, q.ZZZ), PPP)};
+    F PP = csqr(P);
+    F PPP = cmul(P, PP);
+    F Q = cmul(U1, PP);
+    F X3 = sub(sub(csqr(R), PPP), dbl(Q));
+    F Y3 = sub(cmul(R, sub(Q, X3)), cmul(S1, PPP));
+    return {X3, Y3, cmul(cmul(p.ZZ, q.ZZ), PP), cmul(cmul(p.ZZZ, q.ZZZ), PPP)};
 }
 
 template <class F> __device__ __forceinline__ XYZZ<F> xyzz_neg(const XYZZ<F>& p) { return {p.X, neg(p.Y), p.ZZ, p.ZZZ}; }
@@ -145,19 +161,19 @@ template <class F> __device__ __forceinline__ XYZZ<F> xyzz_neg(const XYZZ<F>& p)
 template <class F> __device__ __forceinline__ Jac<F> xyzz_to_jac(const XYZZ<F>& p)
 {
     if (xyzz_is_inf(p)) return {F::zero(), F::one(), F::zero()};
-    F zzz2 = sqr(p.ZZZ);
-    F Z = mul(p.ZZ, p.ZZZ);
-    F X = mul(mul(p.X, p.ZZ), zzz2);
-    F zz3 = mul(sqr(p.ZZ), p.ZZ);
-    F Y = mul(mul(p.Y, zz3), zzz2);
+    F zzz2 = csqr(p.ZZZ);
+    F Z = cmul(p.ZZ, p.ZZZ);
+    F X = cmul(cmul(p.X, p.ZZ), zzz2);
+    F zz3 = cmul(csqr(p.ZZ), p.ZZ);
+    F Y = cmul(cmul(p.Y, zz3), zzz2);
     return {X, Y, Z};
 }
 
 template <class F> __device__ __forceinline__ XYZZ<F> jac_to_xyzz(const Jac<F>& p)
 {
     if (p.Z.is_zero()) return xyzz_inf<F>();
-    F z2 = sqr(p.Z);
-    return {p.X, p.Y, z2, mul(z2, p.Z)};
+    F z2 = csqr(p.Z);
+    return {p.X, p.Y, z2, cmul(z2, p.Z)};
 }
 
 // Out-of-line copies for the cold kernels (fix-up, reduction levels, window

@@ -238,6 +238,12 @@ __device__ __forceinline__ Fp<P> mul(const Fp<P>& a, const Fp<P>& b)
 
 template <class P> __device__ __forceinline__ Fp<P> sqr(const Fp<P>& a) { return mul(a, a); }
 
+// Out-of-line Montgomery product for code that chains many products (the
+// curve formulas): one ~300-instruction body shared by every call keeps the
+// hot loops inside the instruction cache, where fully inlined mixed
+// additions (ten products each) would not fit.
+template <class P> __device__ __noinline__ Fp<P> mul_call(const Fp<P> a, const Fp<P> b) { return mul(a, b); }
+
 // Montgomery -> canonical integer (multiply by 1)
 template <class P>
 __device__ __forceinline__ Fp<P> from_mont(const Fp<P>& a)

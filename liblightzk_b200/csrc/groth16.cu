@@ -6,8 +6,10 @@
 // fixed sequence of launches on three streams with no host round trip:
 //
 //   stream main : SpMV A z, B z, C z -> H polynomial -> H MSM -> assembly
-//   stream s1   : A MSM, B1 MSM -> s*Ar, r*Bs1 -> L MSM
-//   stream s2   : r*d1, s*d1, (-r s)*d1, s*d2 -> B2 MSM (G2)
+//   stream s1   : A MSM, B1 MSM, L MSM
+//   stream s2   : B2 MSM (G2)
+//   stream s3   : fixed-point products r d1, s a1, r b1, (r s) d1, s d2 from
+//                 comb tables; after B1: s*A and r*B1 (variable base)
 //
 // H polynomial, two modes:
 //   LZK_PROVE_REFERENCE reproduces the reference chain exactly
@@ -18,13 +20,18 @@
 //   LZK_PROVE_STANDARD is the standard quotient on the coset g<w_M>:
 //     iNTT_M, coset NTT_M, (A*B - C) * (g^M - 1)^-1, coset iNTT_M,
 //     H scalars = h_0 .. h_{M-2}; all transforms stay at size M.
-// Phase 6 (groth16.cuh:211-215) runs on the device:
+// Phase 6 (groth16.cuh:211-215) runs on the device.  The reference forms
 //   Ar = a1 + A + r d1,  Bs1 = b1 + B1 + s d1,  Bs2 = b2 + B2 + s d2,
-//   Krs = s Ar + r Bs1 + (-r s) d1 + L,  proof = (Ar, Bs2, Krs + H).
+//   Krs = s Ar + r Bs1 + (-r s) d1 + L,  proof = (Ar, Bs2, Krs + H);
+// expanding s Ar and r Bs1 gives the same group element
+//   Krs + H = s a1 + r b1 + s A + r B1 + (r s) d1 + L + H,
+// whose fixed-base terms come from per-prover comb tables (32 mixed
+// additions each) and whose only variable-base products are s A and r B1.
 #include "common.cuh"
 #include "curve.cuh"
 #include "msm.cuh"
 #include "ntt.cuh"
+#include "keygen.cuh"
 #include "r1cs.cuh"
 #include <new>
 
@@ -49,12 +56,14 @@ struct lzk_prover {
     size_t L = 0;
     lzk::Jac<lzk::Fq>* g1res = nullptr;   // A, B1, L, H MSM results
     lzk::Jac<lzk::Fq2>* g2res = nullptr;  // B2 MSM result
-    lzk::XYZZ<lzk::Fq>* sm1 = nullptr;    // r d1, s d1, (-rs) d1, s Ar, r Bs1
+    lzk::XYZZ<lzk::Fq>* sm1 = nullptr;    // r d1, s a1, r b1, (r s) d1, s A, r B1
     lzk::XYZZ<lzk::Fq2>* sm2 = nullptr;   // s d2
+    lzk::Aff<lzk::Fq>* comb1 = nullptr;   // comb tables of a1, b1, d1 (3 x 8192)
+    lzk::Aff<lzk::Fq2>* comb2 = nullptr;  // comb table of d2
     void* ws[3] = {nullptr, nullptr, nullptr};
     size_t wsb[3] = {0, 0, 0};
-    cudaStream_t s1 = nullptr, s2 = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_fixed = nullptr, ev_s1 = nullptr, ev_s2 = nullptr;
+    cudaStream_t s1 = nullptr, s2 = nullptr, s3 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_b1 = nullptr, ev_s1 = nullptr, ev_s2 = nullptr, ev_s3 = nullptr;
     size_t bytes = 0;
 };
 
@@ -73,57 +82,66 @@ __device__ __forceinline__ Fr canon(const Scal& s)
     return from_mont(m);
 }
 
-// k * P by MSB-first double-and-add over 256 bits (curve_utils.cuh:28-49)
+// k * P, 4-bit fixed window: 15 precomputed multiples, then per nibble four
+// doublings and one addition (curve_utils.cuh:28-49 computes the same
+// product bit by bit)
 template <class F>
-__device__ XYZZ<F> smul(const XYZZ<F>& P, const Fr& k)
+__device__ XYZZ<F> smul_w4(const XYZZ<F>& P, const Fr& k)
 {
+    XYZZ<F> tab[16];
+    tab[0] = xyzz_inf<F>();
+    tab[1] = P;
+    for (int i = 2; i < 16; i++) tab[i] = (i & 1) ? xyzz_add_cold(tab[i - 1], P) : xyzz_dbl_cold(tab[i >> 1]);
     XYZZ<F> acc = xyzz_inf<F>();
-    for (int i = 255; i >= 0; i--) {
-        acc = xyzz_dbl_cold(acc);
-        if ((k.v[i >> 5] >> (i & 31)) & 1) acc = xyzz_add_cold(acc, P);
+    for (int w = 63; w >= 0; w--) {
+        for (int d = 0; d < 4; d++) acc = xyzz_dbl_cold(acc);
+        uint32_t nib = (k.v[w >> 3] >> (4 * (w & 7))) & 15u;
+        if (nib) acc = xyzz_add_cold(acc, tab[nib]);
     }
     return acc;
 }
 
-// the fixed-point products: thread 0 r d1, 1 s d1, 2 (-r s) d1, 3 s d2
-__global__ void k_fixed_smuls(const Aff<Fq>* g1c, const Aff<Fq2>* g2c, Scal r, Scal s, XYZZ<Fq>* sm1, XYZZ<Fq2>* sm2)
+// fixed-base products from comb tables: thread 0 r d1, 1 s a1, 2 r b1,
+// 3 (r s) d1, 4 s d2
+__global__ void k_fixed_products(const Aff<Fq>* __restrict__ comb1, const Aff<Fq2>* __restrict__ comb2, Scal r, Scal s,
+                                 XYZZ<Fq>* __restrict__ sm1, XYZZ<Fq2>* __restrict__ sm2)
 {
     uint32_t t = threadIdx.x;
-    if (t < 3) {
-        Fr rm, sm;
-        _Pragma("unroll") for (int i = 0; i < 8; i++) { rm.v[i] = r.v[i]; sm.v[i] = s.v[i]; }
-        Fr k = t == 0 ? rm : (t == 1 ? sm : mul(neg(rm), sm));
-        sm1[t] = smul(xyzz_from_aff(g1c[2]), from_mont(k));
-    } else if (t == 3) {
-        sm2[0] = smul(xyzz_from_aff(g2c[1]), canon(s));
-    }
+    if (t > 4) return;
+    Fr rm, sm;
+    _Pragma("unroll") for (int i = 0; i < 8; i++) { rm.v[i] = r.v[i]; sm.v[i] = s.v[i]; }
+    if (t == 4) { sm2[0] = comb_mul(comb2, from_mont(sm)); return; }
+    const int table[4] = {2, 0, 1, 2};   // d1, a1, b1, d1
+    Fr k = t == 0 ? rm : t == 1 ? sm : t == 2 ? rm : mul(rm, sm);
+    sm1[t] = comb_mul(comb1 + table[t] * 8192, from_mont(k));
 }
 
-// thread 0: s * Ar, Ar = a1 + A + r d1; thread 1: r * Bs1, Bs1 = b1 + B1 + s d1
-__global__ void k_dep_smuls(const Aff<Fq>* g1c, const Jac<Fq>* g1res, Scal r, Scal s, XYZZ<Fq>* sm1)
+// variable-base products: thread 0 s * A, thread 1 r * B1
+__global__ void k_dep_products(const Jac<Fq>* __restrict__ g1res, Scal r, Scal s, XYZZ<Fq>* __restrict__ sm1)
 {
     uint32_t t = threadIdx.x;
     if (t > 1) return;
-    XYZZ<Fq> base = xyzz_from_aff(g1c[t]);
-    base = xyzz_add_cold(base, jac_to_xyzz(g1res[t]));
-    base = xyzz_add_cold(base, sm1[t]);
-    sm1[3 + t] = smul(base, canon(t == 0 ? s : r));
+    sm1[4 + t] = smul_w4(jac_to_xyzz(g1res[t]), canon(t == 0 ? s : r));
 }
 
-// proof.A = Ar, proof.C = s Ar + r Bs1 + (-rs) d1 + L + H, proof.B = b2 + B2 + s d2
+// proof.A = a1 + A + r d1; proof.B = b2 + B2 + s d2;
+// proof.C = s a1 + r b1 + (r s) d1 + s A + r B1 + L + H
 __global__ void k_assemble(const Aff<Fq>* g1c, const Aff<Fq2>* g2c, const Jac<Fq>* g1res, const Jac<Fq2>* g2res,
                            const XYZZ<Fq>* sm1, const XYZZ<Fq2>* sm2, lzk_groth16_proof* proof)
 {
     uint32_t t = threadIdx.x;
     if (t == 0) {
-        XYZZ<Fq> Ar = xyzz_add_cold(xyzz_add_cold(xyzz_from_aff(g1c[0]), jac_to_xyzz(g1res[0])), sm1[0]);
-        XYZZ<Fq> C = xyzz_add_cold(sm1[3], sm1[4]);
-        C = xyzz_add_cold(C, sm1[2]);
+        XYZZ<Fq> A = xyzz_add_cold(xyzz_add_cold(xyzz_from_aff(g1c[0]), jac_to_xyzz(g1res[0])), sm1[0]);
+        st_elem(reinterpret_cast<Jac<Fq>*>(&proof->A), xyzz_to_jac(A));
+    } else if (t == 1) {
+        XYZZ<Fq> C = xyzz_add_cold(sm1[1], sm1[2]);
+        C = xyzz_add_cold(C, sm1[3]);
+        C = xyzz_add_cold(C, sm1[4]);
+        C = xyzz_add_cold(C, sm1[5]);
         C = xyzz_add_cold(C, jac_to_xyzz(g1res[2]));
         C = xyzz_add_cold(C, jac_to_xyzz(g1res[3]));
-        st_elem(reinterpret_cast<Jac<Fq>*>(&proof->A), xyzz_to_jac(Ar));
         st_elem(reinterpret_cast<Jac<Fq>*>(&proof->C), xyzz_to_jac(C));
-    } else if (t == 1) {
+    } else if (t == 2) {
         XYZZ<Fq2> B = xyzz_add_cold(xyzz_add_cold(xyzz_from_aff(g2c[0]), jac_to_xyzz(g2res[0])), sm2[0]);
         st_elem(reinterpret_cast<Jac<Fq2>*>(&proof->B), xyzz_to_jac(B));
     }
@@ -164,11 +182,12 @@ static void destroy(lzk_prover* p)
     for (auto t : p->tab) if (t) cudaFree(t);
     if (p->tab2) cudaFree(p->tab2);
     for (auto w : p->ws) if (w) cudaFree(w);
-    void* misc[] = {p->g1c, p->g2c, p->zinv, p->x, p->g1res, p->g2res, p->sm1, p->sm2};
+    void* misc[] = {p->g1c, p->g2c, p->zinv, p->x, p->g1res, p->g2res, p->sm1, p->sm2, p->comb1, p->comb2};
     for (auto m : misc) if (m) cudaFree(m);
     if (p->s1) cudaStreamDestroy(p->s1);
     if (p->s2) cudaStreamDestroy(p->s2);
-    cudaEvent_t evs[] = {p->ev_fork, p->ev_fixed, p->ev_s1, p->ev_s2};
+    if (p->s3) cudaStreamDestroy(p->s3);
+    cudaEvent_t evs[] = {p->ev_fork, p->ev_b1, p->ev_s1, p->ev_s2, p->ev_s3};
     for (auto e : evs) if (e) cudaEventDestroy(e);
     delete p;
 }
@@ -204,10 +223,9 @@ static int create(const lzk_groth16_circuit* c, const lzk_groth16_pk* pk, int mo
 
     LZK_CUDA(cudaStreamCreateWithFlags(&p->s1, cudaStreamNonBlocking));
     LZK_CUDA(cudaStreamCreateWithFlags(&p->s2, cudaStreamNonBlocking));
-    LZK_CUDA(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
-    LZK_CUDA(cudaEventCreateWithFlags(&p->ev_fixed, cudaEventDisableTiming));
-    LZK_CUDA(cudaEventCreateWithFlags(&p->ev_s1, cudaEventDisableTiming));
-    LZK_CUDA(cudaEventCreateWithFlags(&p->ev_s2, cudaEventDisableTiming));
+    LZK_CUDA(cudaStreamCreateWithFlags(&p->s3, cudaStreamNonBlocking));
+    cudaEvent_t* evs[] = {&p->ev_fork, &p->ev_b1, &p->ev_s1, &p->ev_s2, &p->ev_s3};
+    for (auto e : evs) LZK_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     cudaStream_t st = p->s1;
 
     // tables
@@ -231,14 +249,18 @@ static int create(const lzk_groth16_circuit* c, const lzk_groth16_pk* pk, int mo
     LZK_CUDA(cudaMemcpyAsync(p->g1c, g1h, sizeof(g1h), cudaMemcpyHostToDevice, st));
     LZK_CUDA(cudaMemcpyAsync(p->g2c, g2h, sizeof(g2h), cudaMemcpyHostToDevice, st));
     LZK_TRY(dalloc(p, &p->zinv, 1));
-    k_zinv<<<1, 32, 0, st>>>(p->log_m, p->zinv);
+    k_zinv<<<1, 32, 0, st>>>(p->log_m, p->zinv); note_launch();
 
     // scratch
     p->L = mode == LZK_PROVE_REFERENCE ? 2 * p->M : p->M;
     LZK_TRY(dalloc(p, &p->x, 3 * p->L));
     LZK_TRY(dalloc(p, &p->g1res, 4));
     LZK_TRY(dalloc(p, &p->g2res, 1));
-    LZK_TRY(dalloc(p, &p->sm1, 5));
+    LZK_TRY(dalloc(p, &p->sm1, 6));
+    LZK_TRY(dalloc(p, &p->comb1, 3 * 8192));
+    LZK_TRY(dalloc(p, &p->comb2, 8192));
+    for (int i = 0; i < 3; i++) LZK_TRY(comb_build<Fq>(p->g1c + i, p->comb1 + i * 8192, st));
+    LZK_TRY(comb_build<Fq2>(p->g2c + 1, p->comb2, st));
     LZK_TRY(dalloc(p, &p->sm2, 1));
     for (int i = 0; i < 3; i++) {
         lzk_msm_cfg cfg{};
@@ -284,10 +306,12 @@ static int prove(lzk_prover* p, const Fr* z, const lzk_fr_t* r, const lzk_fr_t* 
     LZK_CUDA(cudaEventRecord(p->ev_fork, st));
     LZK_CUDA(cudaStreamWaitEvent(p->s1, p->ev_fork, 0));
     LZK_CUDA(cudaStreamWaitEvent(p->s2, p->ev_fork, 0));
+    LZK_CUDA(cudaStreamWaitEvent(p->s3, p->ev_fork, 0));
 
-    // s2: fixed-point scalar products, then the G2 MSM
-    k_fixed_smuls<<<1, 32, 0, p->s2>>>(p->g1c, p->g2c, rs, ss, p->sm1, p->sm2);
-    LZK_CUDA(cudaEventRecord(p->ev_fixed, p->s2));
+    // s3: fixed-base products
+    k_fixed_products<<<1, 32, 0, p->s3>>>(p->comb1, p->comb2, rs, ss, p->sm1, p->sm2); note_launch();
+
+    // s2: the G2 MSM
     {
         lzk_msm_cfg cfg{};
         cfg.window_bits = p->c;
@@ -301,11 +325,13 @@ static int prove(lzk_prover* p, const Fr* z, const lzk_fr_t* r, const lzk_fr_t* 
     }
     LZK_CUDA(cudaEventRecord(p->ev_s2, p->s2));
 
-    // s1: A, B1 MSMs, dependent products, L MSM
+    // s1: A, B1 and L MSMs; s3 picks up A and B1 for s*A and r*B1
     LZK_TRY(msm_tab1(p, 0, z, p->n_vars, p->g1res + 0, 1, p->s1));
     LZK_TRY(msm_tab1(p, 1, z, p->n_vars, p->g1res + 1, 1, p->s1));
-    LZK_CUDA(cudaStreamWaitEvent(p->s1, p->ev_fixed, 0));
-    k_dep_smuls<<<1, 32, 0, p->s1>>>(p->g1c, p->g1res, rs, ss, p->sm1);
+    LZK_CUDA(cudaEventRecord(p->ev_b1, p->s1));
+    LZK_CUDA(cudaStreamWaitEvent(p->s3, p->ev_b1, 0));
+    k_dep_products<<<1, 32, 0, p->s3>>>(p->g1res, rs, ss, p->sm1); note_launch();
+    LZK_CUDA(cudaEventRecord(p->ev_s3, p->s3));
     size_t nl = p->n_vars - p->n_public - 1;
     LZK_TRY(msm_tab1(p, 2, z + p->n_public + 1, nl, p->g1res + 2, 1, p->s1));
     LZK_CUDA(cudaEventRecord(p->ev_s1, p->s1));
@@ -329,7 +355,7 @@ static int prove(lzk_prover* p, const Fr* z, const lzk_fr_t* r, const lzk_fr_t* 
     if (p->mode == LZK_PROVE_REFERENCE) {
         LZK_TRY(ntt_run(p->x, p->log_m, LZK_NTT_INVERSE, 3, p->L, nullptr, st));
         LZK_TRY(ntt_run(p->x, p->log_m + 1, LZK_NTT_FORWARD, 3, p->L, nullptr, st));
-        k_abc<<<grid_for(p->L, 256, 148 * 8), 256, 0, st>>>(x0, x1, x2, p->L, nullptr);
+        k_abc<<<grid_for(p->L, 256, 148 * 8), 256, 0, st>>>(x0, x1, x2, p->L, nullptr); note_launch();
         NttTables t4; CosetTables ct;
         LZK_TRY(get_tables(p->log_m + 2, t4, ct));
         LZK_TRY(ntt_run(x0, p->log_m + 1, LZK_NTT_INVERSE, 1, 0, t4.consts + 2, st));
@@ -337,7 +363,7 @@ static int prove(lzk_prover* p, const Fr* z, const lzk_fr_t* r, const lzk_fr_t* 
     } else {
         LZK_TRY(ntt_run(p->x, p->log_m, LZK_NTT_INVERSE, 3, p->L, nullptr, st));
         LZK_TRY(ntt_run(p->x, p->log_m, LZK_NTT_COSET_FORWARD, 3, p->L, nullptr, st));
-        k_abc<<<grid_for(p->L, 256, 148 * 8), 256, 0, st>>>(x0, x1, x2, p->L, p->zinv);
+        k_abc<<<grid_for(p->L, 256, 148 * 8), 256, 0, st>>>(x0, x1, x2, p->L, p->zinv); note_launch();
         LZK_TRY(ntt_run(x0, p->log_m, LZK_NTT_COSET_INVERSE, 1, 0, nullptr, st));
         hs = x0;
     }
@@ -346,7 +372,8 @@ static int prove(lzk_prover* p, const Fr* z, const lzk_fr_t* r, const lzk_fr_t* 
     // join and assemble
     LZK_CUDA(cudaStreamWaitEvent(st, p->ev_s1, 0));
     LZK_CUDA(cudaStreamWaitEvent(st, p->ev_s2, 0));
-    k_assemble<<<1, 32, 0, st>>>(p->g1c, p->g2c, p->g1res, p->g2res, p->sm1, p->sm2, proof);
+    LZK_CUDA(cudaStreamWaitEvent(st, p->ev_s3, 0));
+    k_assemble<<<1, 32, 0, st>>>(p->g1c, p->g2c, p->g1res, p->g2res, p->sm1, p->sm2, proof); note_launch();
     trace_end(tr, st);
     return launch_status();
 }

@@ -12,8 +12,7 @@
 // the 32 entries selected by the bytes of k -- 32 mixed XYZZ additions per
 // scalar and no doublings; results are normalised to affine with one
 // inversion per 8 points.
-#include "common.cuh"
-#include "curve.cuh"
+#include "keygen.cuh"
 #include <map>
 #include <mutex>
 
@@ -85,12 +84,13 @@ template <> __device__ Aff<Fq2> generator<Fq2>()
     return {Fq2{x0, x1}, Fq2{y0, y1}};
 }
 
-// base_j = 2^(8j) G for j < 32 (one thread, 248 doublings)
+// base_j = 2^(8j) P for j < 32 (one thread, 248 doublings); P = the
+// generator when base is null
 template <class F>
-__global__ void k_comb_bases(XYZZ<F>* __restrict__ bases)
+__global__ void k_comb_bases(const Aff<F>* __restrict__ base, XYZZ<F>* __restrict__ bases)
 {
     if (gtid() != 0) return;
-    XYZZ<F> b = xyzz_from_aff(generator<F>());
+    XYZZ<F> b = xyzz_from_aff(base ? *base : generator<F>());
     for (int j = 0; j < 32; j++) {
         st_elem(bases + j, b);
         for (int d = 0; d < 8; d++) b = xyzz_dbl_cold(b);
@@ -144,16 +144,22 @@ template <class F>
 __global__ void __launch_bounds__(128) k_fixed_base(const Fr* __restrict__ k, size_t n, const Aff<F>* __restrict__ T,
                                                      XYZZ<F>* __restrict__ out)
 {
-    for (uint64_t i = gtid(); i < n; i += gstride()) {
-        Fr s = from_mont(ldg_elem(k + i));
-        XYZZ<F> acc = xyzz_inf<F>();
-        for (int j = 0; j < 32; j++) {
-            uint32_t d = (s.v[j >> 2] >> (8 * (j & 3))) & 255u;
-            if (d) acc = xyzz_madd(acc, ldg_elem(T + j * 256 + d));
-        }
-        st_elem(out + i, acc);
-    }
+    for (uint64_t i = gtid(); i < n; i += gstride()) st_elem(out + i, comb_mul(T, from_mont(ldg_elem(k + i))));
 }
+
+template <class F>
+int comb_build(const Aff<F>* base, Aff<F>* T, cudaStream_t st)
+{
+    Scratch ws;
+    LZK_TRY(ws.acquire((32 * 256 + 32) * sizeof(XYZZ<F>), nullptr, 0, st));
+    XYZZ<F>* tmp = reinterpret_cast<XYZZ<F>*>(ws.base);
+    k_comb_bases<F><<<1, 32, 0, st>>>(base, tmp + 32 * 256); note_launch();
+    k_comb_fill<F><<<64, 128, 0, st>>>(tmp + 32 * 256, tmp); note_launch();
+    k_xyzz_to_aff<F><<<grid_for(32 * 256 / 8, 128), 128, 0, st>>>(tmp, T, 32 * 256); note_launch();
+    return launch_status();
+}
+template int comb_build<Fq>(const Aff<Fq>*, Aff<Fq>*, cudaStream_t);
+template int comb_build<Fq2>(const Aff<Fq2>*, Aff<Fq2>*, cudaStream_t);
 
 static std::mutex g_comb_mu;
 static std::map<int, void*> g_comb[3];
@@ -167,21 +173,12 @@ static int comb_table(const Aff<F>** out, int group)
     auto it = g_comb[group].find(dev);
     if (it != g_comb[group].end()) { *out = static_cast<const Aff<F>*>(it->second); return LZK_OK; }
     Aff<F>* T = nullptr;
-    XYZZ<F>* tmp = nullptr;
-    if (cudaMalloc(&T, 32 * 256 * sizeof(Aff<F>)) != cudaSuccess ||
-        cudaMalloc(&tmp, (32 * 256 + 32) * sizeof(XYZZ<F>)) != cudaSuccess) {
-        cudaGetLastError();
-        if (T) cudaFree(T);
-        return LZK_ENOMEM;
-    }
+    if (cudaMalloc(&T, 32 * 256 * sizeof(Aff<F>)) != cudaSuccess) { cudaGetLastError(); return LZK_ENOMEM; }
     cudaStream_t st;
     LZK_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    k_comb_bases<F><<<1, 32, 0, st>>>(tmp + 32 * 256);
-    k_comb_fill<F><<<64, 128, 0, st>>>(tmp + 32 * 256, tmp);
-    k_xyzz_to_aff<F><<<grid_for(32 * 256 / 8, 128), 128, 0, st>>>(tmp, T, 32 * 256);
-    int rc = cuda_status(cudaStreamSynchronize(st));
+    int rc = comb_build<F>(nullptr, T, st);
+    if (rc == LZK_OK) rc = cuda_status(cudaStreamSynchronize(st));
     cudaStreamDestroy(st);
-    cudaFree(tmp);
     if (rc != LZK_OK) { cudaFree(T); return rc; }
     g_comb[group][dev] = T;
     *out = T;
@@ -198,8 +195,8 @@ static int fixed_base(const Fr* k, size_t n, Aff<F>* out, int group, cudaStream_
     Scratch ws;
     LZK_TRY(ws.acquire(n * sizeof(XYZZ<F>), nullptr, 0, st));
     XYZZ<F>* tmp = reinterpret_cast<XYZZ<F>*>(ws.base);
-    k_fixed_base<F><<<grid_for(n, 128), 128, 0, st>>>(k, n, T, tmp);
-    k_xyzz_to_aff<F><<<grid_for((n + 7) / 8, 128), 128, 0, st>>>(tmp, out, n);
+    k_fixed_base<F><<<grid_for(n, 128), 128, 0, st>>>(k, n, T, tmp); note_launch();
+    k_xyzz_to_aff<F><<<grid_for((n + 7) / 8, 128), 128, 0, st>>>(tmp, out, n); note_launch();
     return launch_status();
 }
 
@@ -214,7 +211,7 @@ int lzk_random_fr(uint64_t seed, uint64_t stream_id, uint64_t offset, size_t n, 
     if (!n) return LZK_OK;
     if (!out) return LZK_EINVAL;
     k_random_fr<<<grid_for(n, 256, 148 * 16), 256, 0, as_stream(stream)>>>(seed, stream_id, offset, n,
-                                                                         reinterpret_cast<Fr*>(out));
+                                                                         reinterpret_cast<Fr*>(out)); note_launch();
     return launch_status();
 }
 

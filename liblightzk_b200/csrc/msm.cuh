@@ -11,7 +11,7 @@ struct G2 { using F = Fq2; };
 
 constexpr uint32_t kAccChunk = 32;   // sorted entries per accumulation thread
 constexpr uint32_t kLevelL = 8;      // buckets per thread in a reduction level
-constexpr uint32_t kFixSmall = 8;    // partials a single fix-up thread folds
+constexpr uint32_t kFixSmall = 64;   // partials a single fix-up thread folds
 
 struct MsmPlan {
     size_t n = 0;
@@ -53,7 +53,7 @@ inline void plan_msm(MsmPlan& p, size_t n, uint32_t c, bool shared, size_t strid
     p.o_lr1 = cv.take<X>(lvl);
     p.o_la1 = cv.take<X>(lvl);
     p.o_scan = cv.take<uint32_t>((p.B + 4095) / 4096 + 1);
-    p.o_large = cv.take<uint32_t>(p.chunks / 8 + 2);   // count, then bucket ids
+    p.o_large = cv.take<uint32_t>(p.chunks / kFixSmall + 2);   // count, then bucket ids
     p.bytes = cv.off;
 }
 
@@ -82,8 +82,9 @@ __device__ __forceinline__ Aff<F> load_base(const Aff<F>* bases, uint32_t v)
     return p;
 }
 
+// 128-thread blocks; at most 102 registers for G1 (5 blocks = 20 warps per SM)
 template <class F>
-__global__ void __launch_bounds__(256) k_accumulate(const Aff<F>* __restrict__ bases, const uint32_t* __restrict__ ent,
+__global__ void __launch_bounds__(128, sizeof(F) == 32 ? 5 : 2) k_accumulate(const Aff<F>* __restrict__ bases, const uint32_t* __restrict__ ent,
                                                     const uint32_t* __restrict__ off, uint32_t B, size_t chunks,
                                                     XYZZ<F>* __restrict__ bsum, XYZZ<F>* __restrict__ head,
                                                     XYZZ<F>* __restrict__ tail)
@@ -227,7 +228,7 @@ int run_msm(const Fr* scalars, const Aff<typename Gp::F>* bases, size_t n, Jac<t
         if ((size_t)windows_for(c) * stride >= (1ull << 31)) return LZK_EINVAL;
     }
     if (n == 0) {
-        k_write_inf<F><<<1, 32, 0, st>>>(out);
+        k_write_inf<F><<<1, 32, 0, st>>>(out); note_launch();
         return launch_status();
     }
     MsmPlan p;
@@ -249,13 +250,13 @@ int run_msm(const Fr* scalars, const Aff<typename Gp::F>* bases, size_t n, Jac<t
     uint32_t* large = reinterpret_cast<uint32_t*>(base + p.o_large);
     LZK_TRY(msm_sort(p, scalars, cnt, off, ent, bsums, st));
     void* tr = trace_begin(sizeof(F) == 32 ? "msm_g1_accumulate" : "msm_g2_accumulate", st);
-    k_accumulate<F><<<grid_for(p.chunks, 256), 256, 0, st>>>(bases, ent, off, p.B, p.chunks, bsum, head, tail);
+    k_accumulate<F><<<grid_for(p.chunks, 128), 128, 0, st>>>(bases, ent, off, p.B, p.chunks, bsum, head, tail); note_launch();
     trace_end(tr, st);
     LZK_CUDA(cudaMemsetAsync(large, 0, sizeof(uint32_t), st));
-    k_fixup<F><<<grid_for(p.B, 256, 148 * 8), 256, 0, st>>>(off, p.B, bsum, head, tail, large);
+    k_fixup<F><<<grid_for(p.B, 256, 148 * 8), 256, 0, st>>>(off, p.B, bsum, head, tail, large); note_launch();
     {
         constexpr unsigned fx_threads = 32768 / sizeof(X);   // 32 KB of shared memory
-        k_fixup_large<F><<<148 * 2, fx_threads, fx_threads * sizeof(X), st>>>(off, bsum, head, tail, large);
+        k_fixup_large<F><<<148 * 2, fx_threads, fx_threads * sizeof(X), st>>>(off, bsum, head, tail, large); note_launch();
     }
     LZK_TRY(launch_status());
 
@@ -267,7 +268,7 @@ int run_msm(const Fr* scalars, const Aff<typename Gp::F>* bases, size_t n, Jac<t
         uint32_t L = m < kLevelL ? m : kLevelL;
         uint32_t segs = m / L;
         size_t threads = (size_t)p.wb * segs;
-        k_level<F><<<grid_for(threads, 128), 128, 0, st>>>(inR, inA, offp, p.wb, m, L, base1, logM, lr[pp], la[pp]);
+        k_level<F><<<grid_for(threads, 128), 128, 0, st>>>(inR, inA, offp, p.wb, m, L, base1, logM, lr[pp], la[pp]); note_launch();
         inR = lr[pp]; inA = la[pp]; resA = la[pp];
         offp = nullptr; base1 = 0;
         uint32_t lg = 0; while ((1u << lg) < L) lg++;
@@ -276,7 +277,7 @@ int run_msm(const Fr* scalars, const Aff<typename Gp::F>* bases, size_t n, Jac<t
         pp ^= 1;
         if (m == 1) break;
     }
-    k_finish<F><<<1, 32, 0, st>>>(resA, p.wb, c, out);
+    k_finish<F><<<1, 32, 0, st>>>(resA, p.wb, c, out); note_launch();
     trace_end(tr_all, st);
     return launch_status();
 }
@@ -353,7 +354,7 @@ int run_precompute(const Aff<F>* bases, size_t n, uint32_t c, uint32_t windows, 
 {
     if (!bases || !table || c < 2 || c > 24 || windows == 0 || windows > 256 || stride < n) return LZK_EINVAL;
     if (n == 0) return LZK_OK;
-    k_precompute<F><<<grid_for(n, 64), 64, 0, st>>>(bases, n, c, windows, table, stride);
+    k_precompute<F><<<grid_for(n, 64), 64, 0, st>>>(bases, n, c, windows, table, stride); note_launch();
     return launch_status();
 }
 

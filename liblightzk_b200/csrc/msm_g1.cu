@@ -26,7 +26,7 @@ int lzk_g1_to_affine(const lzk_g1_t* in, lzk_g1_affine_t* out, size_t n, void* s
     if ((!in || !out) && n) return LZK_EINVAL;
     if (!n) return LZK_OK;
     k_jac_to_aff<Fq><<<grid_for((n + 7) / 8, 128), 128, 0, as_stream(stream)>>>(
-        reinterpret_cast<const Jac<Fq>*>(in), reinterpret_cast<Aff<Fq>*>(out), n);
+        reinterpret_cast<const Jac<Fq>*>(in), reinterpret_cast<Aff<Fq>*>(out), n); note_launch();
     return launch_status();
 }
 

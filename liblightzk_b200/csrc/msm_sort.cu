@@ -158,12 +158,12 @@ int msm_sort(const MsmPlan& p, const Fr* scalars, uint32_t* cnt, uint32_t* off, 
 {
     LZK_CUDA(cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * p.B, st));
     unsigned g = grid_for(p.n, 256, 148 * 16);
-    k_count<<<g, 256, 0, st>>>(scalars, p.n, p.c, p.W, p.nb, p.shared, cnt);
+    k_count<<<g, 256, 0, st>>>(scalars, p.n, p.c, p.W, p.nb, p.shared, cnt); note_launch();
     uint32_t nblk = (p.B + kScanBlock - 1) / kScanBlock;
-    k_scan_local<<<nblk, 1024, 0, st>>>(cnt, p.B, off, bsums);
-    k_scan_top<<<1, 1024, 0, st>>>(bsums, nblk, off, p.B);
-    k_scan_add<<<grid_for(p.B, 256, 148 * 8), 256, 0, st>>>(off, p.B, bsums);
-    k_scatter<<<g, 256, 0, st>>>(scalars, p.n, p.c, p.W, p.nb, p.shared, p.stride, off, cnt, ent);
+    k_scan_local<<<nblk, 1024, 0, st>>>(cnt, p.B, off, bsums); note_launch();
+    k_scan_top<<<1, 1024, 0, st>>>(bsums, nblk, off, p.B); note_launch();
+    k_scan_add<<<grid_for(p.B, 256, 148 * 8), 256, 0, st>>>(off, p.B, bsums); note_launch();
+    k_scatter<<<g, 256, 0, st>>>(scalars, p.n, p.c, p.W, p.nb, p.shared, p.stride, off, cnt, ent); note_launch();
     return launch_status();
 }
 

@@ -104,9 +104,9 @@ int get_tables(uint32_t k, NttTables& out, CosetTables& cos)
             cudaGetLastError();
             rc = LZK_ENOMEM;
         } else {
-            k_ntt_consts<<<1, 32, 0, st>>>(k, t.consts);
-            k_powers<<<grid_for((half + 63) / 64, 128), 128, 0, st>>>(t.consts + 0, t.tw[0], half);
-            k_powers<<<grid_for((half + 63) / 64, 128), 128, 0, st>>>(t.consts + 1, t.tw[1], half);
+            k_ntt_consts<<<1, 32, 0, st>>>(k, t.consts); note_launch();
+            k_powers<<<grid_for((half + 63) / 64, 128), 128, 0, st>>>(t.consts + 0, t.tw[0], half); note_launch();
+            k_powers<<<grid_for((half + 63) / 64, 128), 128, 0, st>>>(t.consts + 1, t.tw[1], half); note_launch();
             rc = cuda_status(cudaStreamSynchronize(st));
             if (rc == LZK_OK) g_ntt_tables[{dev, k}] = t;
         }
@@ -121,8 +121,8 @@ int get_tables(uint32_t k, NttTables& out, CosetTables& cos)
         if (!ok) { cudaGetLastError(); rc = LZK_ENOMEM; }
         else {
             for (int d = 0; d < 2; d++) {
-                k_powers<<<grid_for(nlo / 64, 128), 128, 0, st>>>(cst + 3 + d, c.lo[d], nlo);
-                k_powers<<<grid_for(nhi / 64, 128), 128, 0, st>>>(cst + 5 + d, c.hi[d], nhi);
+                k_powers<<<grid_for(nlo / 64, 128), 128, 0, st>>>(cst + 3 + d, c.lo[d], nlo); note_launch();
+                k_powers<<<grid_for(nhi / 64, 128), 128, 0, st>>>(cst + 5 + d, c.hi[d], nhi); note_launch();
             }
             rc = cuda_status(cudaStreamSynchronize(st));
             if (rc == LZK_OK) g_coset_tables[dev] = c;
@@ -229,7 +229,7 @@ static int ntt_enqueue(Fr* data, uint32_t k, uint32_t count, size_t bstride, con
     }
     if (k == 0) {
         if (scale || post_lo || pre_lo) {
-            k_ntt_bitrev<<<dim3(1, count), 32, 0, st>>>(data, 0, scale, post_lo, post_hi, bstride);
+            k_ntt_bitrev<<<dim3(1, count), 32, 0, st>>>(data, 0, scale, post_lo, post_hi, bstride); note_launch();
             return launch_status();
         }
         return LZK_OK;
@@ -250,10 +250,10 @@ static int ntt_enqueue(Fr* data, uint32_t k, uint32_t count, size_t bstride, con
         size_t blocks = (n >> m) / R;
         size_t smem = (size_t)G * R * sizeof(Fr);
         uint32_t flags = (q == 0 && pre_lo) ? NTT_PRE_COSET : 0u;
-        k_ntt_pass<<<dim3((unsigned)blocks, count), kNttThreads, smem, st>>>(data, pp, tw, flags, pre_lo, pre_hi, bstride);
+        k_ntt_pass<<<dim3((unsigned)blocks, count), kNttThreads, smem, st>>>(data, pp, tw, flags, pre_lo, pre_hi, bstride); note_launch();
         s0 += m;
     }
-    k_ntt_bitrev<<<dim3(grid_for(n, 256, 148 * 8), count), 256, 0, st>>>(data, k, scale, post_lo, post_hi, bstride);
+    k_ntt_bitrev<<<dim3(grid_for(n, 256, 148 * 8), count), 256, 0, st>>>(data, k, scale, post_lo, post_hi, bstride); note_launch();
     return launch_status();
 }
 

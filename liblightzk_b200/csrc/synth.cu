@@ -60,7 +60,7 @@ int lzk_r1cs_solve(const lzk_csr* A, const lzk_csr* B, const lzk_csr* C, lzk_fr_
     if (row_end > a.rows || row_end > b.rows || row_end > c.rows) return LZK_EINVAL;
     if (row_end == row_begin) return LZK_OK;
     k_r1cs_solve<<<grid_for(row_end - row_begin, 128), 128, 0, as_stream(stream)>>>(a, b, c, reinterpret_cast<Fr*>(z),
-                                                                                    row_begin, row_end);
+                                                                                    row_begin, row_end); note_launch();
     return launch_status();
 }
 
@@ -77,7 +77,7 @@ int lzk_r1cs_check(const lzk_csr* A, const lzk_csr* B, const lzk_csr* C, const l
     LZK_CUDA(cudaMemsetAsync(bad_rows, 0, sizeof(unsigned long long), as_stream(stream)));
     if (!rows) return LZK_OK;
     k_r1cs_check<<<grid_for(rows, 128, 148 * 8), 128, 0, as_stream(stream)>>>(a, b, c, reinterpret_cast<const Fr*>(z),
-                                                                             rows, bad_rows);
+                                                                             rows, bad_rows); note_launch();
     return launch_status();
 }
 

@@ -6,6 +6,7 @@
 // every phase; here a traced region only records two events on its stream,
 // and durations are resolved when the host asks for them.
 #include "common.cuh"
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <string>
@@ -22,6 +23,10 @@ static std::mutex g_tr_mu;
 static bool g_tr_on = false;
 static std::vector<TraceRec> g_tr_pending;
 static std::map<std::string, std::pair<double, uint64_t>> g_tr_sum;
+
+static std::atomic<unsigned long long> g_launches{0};
+
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 bool trace_on() { return g_tr_on; }
 
@@ -86,6 +91,8 @@ using namespace lzk;
 
 extern "C" {
 
+uint64_t lzk_launch_count(void) { return g_launches.load(); }
+
 void lzk_trace_enable(int on)
 {
     std::lock_guard<std::mutex> g(g_tr_mu);
@@ -124,9 +131,9 @@ int lzk_probe_imad_rate(double* ops_per_s)
     cudaEventCreate(&a);
     cudaEventCreate(&b);
     const uint32_t iters = 4096, threads = 256, blocks = (uint32_t)sms * 8;
-    k_imad_probe<<<blocks, threads>>>(64, 1u, sink);  // warm-up
+    k_imad_probe<<<blocks, threads>>>(64, 1u, sink); note_launch();  // warm-up
     cudaEventRecord(a);
-    k_imad_probe<<<blocks, threads>>>(iters, 1u, sink);
+    k_imad_probe<<<blocks, threads>>>(iters, 1u, sink); note_launch();
     cudaEventRecord(b);
     cudaError_t e = cudaEventSynchronize(b);
     float ms = 0.f;
