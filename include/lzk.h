@@ -72,21 +72,34 @@ const char* lzk_version(void);
  */
 #define LZK_MSM_PRECOMPUTED 0x1u
 
+/* Layout of the bases (or table entries):
+ *   LZK_BASES_AFFINE        lzk_g1_affine_t / lzk_g2_affine_t
+ *   LZK_BASES_REF_G1_JAC    the reference's G1 records: Jacobian lzk_g1_t
+ *                           (96 B) with Z = 1, as pre_comp_g1 leaves its
+ *                           table (msm.cuh:48-61); Z = 0 is infinity
+ *   LZK_BASES_REF_G2_LANES  the reference's device G2 records: two 96-B
+ *                           halves [X.c0 Y.c0 Z.c0][X.c1 Y.c1 Z.c1] per
+ *                           point (alt_bn128_t.cuh:247-256), Z = 1
+ * so a reference table built by pre_comp_g1/_g2 is consumed in place. */
+#define LZK_BASES_AFFINE        0u
+#define LZK_BASES_REF_G1_JAC    1u
+#define LZK_BASES_REF_G2_LANES  2u
+
 typedef struct lzk_msm_cfg {
     uint32_t window_bits;     /* c; 0 = autotune.  Must equal the table's
                                  window width with LZK_MSM_PRECOMPUTED.     */
     uint32_t flags;           /* LZK_MSM_* */
     uint32_t precomp_windows; /* shifted copies in the table (PRECOMPUTED) */
-    uint32_t reserved;
+    uint32_t base_layout;     /* LZK_BASES_*                                */
     size_t level_stride;      /* points between copies (PRECOMPUTED)        */
     void* workspace;          /* optional device scratch; NULL = allocate
                                  stream-ordered from the device pool        */
     size_t workspace_bytes;
 } lzk_msm_cfg;
 
-int lzk_msm_g1(const lzk_fr_t* scalars, const lzk_g1_affine_t* bases, size_t n,
+int lzk_msm_g1(const lzk_fr_t* scalars, const void* bases, size_t n,
                lzk_g1_t* out, const lzk_msm_cfg* cfg, void* stream);
-int lzk_msm_g2(const lzk_fr_t* scalars, const lzk_g2_affine_t* bases, size_t n,
+int lzk_msm_g2(const lzk_fr_t* scalars, const void* bases, size_t n,
                lzk_g2_t* out, const lzk_msm_cfg* cfg, void* stream);
 /* Scratch bytes lzk_msm_g1/_g2 need for this n and cfg (group 1 or 2). */
 size_t lzk_msm_workspace_bytes(int group, size_t n, const lzk_msm_cfg* cfg);
@@ -149,6 +162,10 @@ typedef struct lzk_csr {
     uint32_t index_bytes;
     uint32_t reserved;
 } lzk_csr;
+
+/* A[i] = A[i] * B[i] - C[i] for i < n (polynomial_A_times_B_minus_C,
+ * poly.cuh:75-85). */
+int lzk_poly_a_times_b_minus_c(lzk_fr_t* A, const lzk_fr_t* B, const lzk_fr_t* C, size_t n, void* stream);
 
 /* Az, Bz, Cz in one launch; a NULL matrix skips its output. */
 int lzk_spmv3(const lzk_csr* A, const lzk_csr* B, const lzk_csr* C, const lzk_fr_t* z,

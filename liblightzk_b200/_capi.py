@@ -33,6 +33,7 @@ SIGNATURES = {
     "lzk_number_theory_transformation": (c_i, [c_sz, c_sz, c_p, c_p, c_p, c_p]),
     "lzk_spmv3": (c_i, [c_p, c_p, c_p, c_p, c_p, c_p, c_p, c_p]),
     "lzk_spmv": (c_i, [c_p, c_p, c_p, c_p]),
+    "lzk_poly_a_times_b_minus_c": (c_i, [c_p, c_p, c_p, c_sz, c_p]),
     "lzk_random_fr": (c_i, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, c_sz, c_p, c_p]),
     "lzk_g1_fixed_base": (c_i, [c_p, c_sz, c_p, c_p]),
     "lzk_g2_fixed_base": (c_i, [c_p, c_sz, c_p, c_p]),
@@ -57,7 +58,7 @@ class MsmCfg(ctypes.Structure):
         ("window_bits", ctypes.c_uint32),
         ("flags", ctypes.c_uint32),
         ("precomp_windows", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32),
+        ("base_layout", ctypes.c_uint32),
         ("level_stride", ctypes.c_size_t),
         ("workspace", ctypes.c_void_p),
         ("workspace_bytes", ctypes.c_size_t),
@@ -65,6 +66,7 @@ class MsmCfg(ctypes.Structure):
 
 
 LZK_MSM_PRECOMPUTED = 0x1
+BASES_AFFINE, BASES_REF_G1_JAC, BASES_REF_G2_LANES = 0, 1, 2
 NTT_FORWARD, NTT_INVERSE, NTT_COSET_FORWARD, NTT_COSET_INVERSE = 0, 1, 2, 3
 
 

@@ -407,6 +407,15 @@ int lzk_prover_destroy(lzk_prover* p)
 
 size_t lzk_prover_device_bytes(const lzk_prover* p) { return p ? p->bytes : 0; }
 
+int lzk_poly_a_times_b_minus_c(lzk_fr_t* A, const lzk_fr_t* B, const lzk_fr_t* C, size_t n, void* stream)
+{
+    if (!n) return LZK_OK;
+    if (!A || !B || !C) return LZK_EINVAL;
+    k_abc<<<grid_for(n, 256, 148 * 8), 256, 0, as_stream(stream)>>>(reinterpret_cast<Fr*>(A), reinterpret_cast<const Fr*>(B),
+                                                                     reinterpret_cast<const Fr*>(C), n, nullptr); note_launch();
+    return launch_status();
+}
+
 int lzk_groth16_prove(lzk_prover* p, const lzk_fr_t* z, const lzk_fr_t* r, const lzk_fr_t* s,
                       lzk_groth16_proof* proof, void* stream)
 {

@@ -74,17 +74,54 @@ __device__ __forceinline__ uint32_t bucket_of(const uint32_t* off, uint32_t lo, 
     return lo;
 }
 
-template <class F>
-__device__ __forceinline__ Aff<F> load_base(const Aff<F>* bases, uint32_t v)
+// Base record layouts (lzk_msm_cfg.base_layout):
+//   LZK_BASES_AFFINE        {x, y}, infinity = (0, 0)
+//   LZK_BASES_REF_G1_JAC    the reference's G1 table records, Jacobian
+//                           {X, Y, Z} (96 B) normalised by pre_comp_g1 to
+//                           Z = 1 (msm.cuh:48-61); Z = 0 is infinity
+//   LZK_BASES_REF_G2_LANES  the reference's device G2 records: two 96-B
+//                           halves {X.c0 Y.c0 Z.c0}{X.c1 Y.c1 Z.c1}
+//                           (alt_bn128_t.cuh:247-256), normalised to Z = 1
+template <class F, int LAYOUT>
+__device__ __forceinline__ Aff<F> load_raw(const void* bases, uint32_t idx);
+
+template <>
+__device__ __forceinline__ Aff<Fq> load_raw<Fq, LZK_BASES_AFFINE>(const void* bases, uint32_t idx)
 {
-    Aff<F> p = ldg_elem(bases + (v & 0x7fffffffu));
+    return ldg_elem(reinterpret_cast<const Aff<Fq>*>(bases) + idx);
+}
+template <>
+__device__ __forceinline__ Aff<Fq2> load_raw<Fq2, LZK_BASES_AFFINE>(const void* bases, uint32_t idx)
+{
+    return ldg_elem(reinterpret_cast<const Aff<Fq2>*>(bases) + idx);
+}
+template <>
+__device__ __forceinline__ Aff<Fq> load_raw<Fq, LZK_BASES_REF_G1_JAC>(const void* bases, uint32_t idx)
+{
+    Jac<Fq> j = ldg_elem(reinterpret_cast<const Jac<Fq>*>(bases) + idx);
+    if (j.Z.is_zero()) return Aff<Fq>{Fq::zero(), Fq::zero()};
+    return Aff<Fq>{j.X, j.Y};
+}
+template <>
+__device__ __forceinline__ Aff<Fq2> load_raw<Fq2, LZK_BASES_REF_G2_LANES>(const void* bases, uint32_t idx)
+{
+    const Jac<Fq>* h = reinterpret_cast<const Jac<Fq>*>(bases) + 2 * (size_t)idx;
+    Jac<Fq> h0 = ldg_elem(h), h1 = ldg_elem(h + 1);
+    if (h0.Z.is_zero() && h1.Z.is_zero()) return Aff<Fq2>{Fq2::zero(), Fq2::zero()};
+    return Aff<Fq2>{Fq2{h0.X, h1.X}, Fq2{h0.Y, h1.Y}};
+}
+
+template <class F, int LAYOUT>
+__device__ __forceinline__ Aff<F> load_base(const void* bases, uint32_t v)
+{
+    Aff<F> p = load_raw<F, LAYOUT>(bases, v & 0x7fffffffu);
     if (v & 0x80000000u) { if (!aff_is_inf(p)) p.y = neg(p.y); }
     return p;
 }
 
 // 128-thread blocks; at most 102 registers for G1 (5 blocks = 20 warps per SM)
-template <class F>
-__global__ void __launch_bounds__(128, sizeof(F) == 32 ? 5 : 2) k_accumulate(const Aff<F>* __restrict__ bases, const uint32_t* __restrict__ ent,
+template <class F, int LAYOUT>
+__global__ void __launch_bounds__(128, sizeof(F) == 32 ? 5 : 2) k_accumulate(const void* __restrict__ bases, const uint32_t* __restrict__ ent,
                                                     const uint32_t* __restrict__ off, uint32_t B, size_t chunks,
                                                     XYZZ<F>* __restrict__ bsum, XYZZ<F>* __restrict__ head,
                                                     XYZZ<F>* __restrict__ tail)
@@ -106,7 +143,7 @@ __global__ void __launch_bounds__(128, sizeof(F) == 32 ? 5 : 2) k_accumulate(con
             bbeg = off[b]; bend = off[b + 1];
             acc = xyzz_inf<F>();
         }
-        acc = xyzz_madd(acc, load_base(bases, ent[e]));
+        acc = xyzz_madd(acc, load_base<F, LAYOUT>(bases, ent[e]));
     }
     bool began_before = bbeg < cs, cont_after = bend > ce;
     if (began_before) st_elem(head + t, acc);
@@ -210,7 +247,7 @@ __global__ void k_write_inf(Jac<F>* out)
 }
 
 template <class Gp>
-int run_msm(const Fr* scalars, const Aff<typename Gp::F>* bases, size_t n, Jac<typename Gp::F>* out,
+int run_msm(const Fr* scalars, const void* bases, size_t n, Jac<typename Gp::F>* out,
                    const lzk_msm_cfg* cfg, cudaStream_t st, uint32_t c_auto)
 {
     using F = typename Gp::F;
@@ -218,6 +255,9 @@ int run_msm(const Fr* scalars, const Aff<typename Gp::F>* bases, size_t n, Jac<t
     if (!out || (n && (!scalars || !bases))) return LZK_EINVAL;
     if (n >= (1ull << 31)) return LZK_EINVAL;
     uint32_t flags = cfg ? cfg->flags : 0u;
+    uint32_t layout = cfg ? cfg->base_layout : (uint32_t)LZK_BASES_AFFINE;
+    uint32_t ref_layout = sizeof(F) == 32 ? LZK_BASES_REF_G1_JAC : LZK_BASES_REF_G2_LANES;
+    if (layout != LZK_BASES_AFFINE && layout != ref_layout) return LZK_EINVAL;
     bool shared = (flags & LZK_MSM_PRECOMPUTED) != 0;
     uint32_t c = (cfg && cfg->window_bits) ? cfg->window_bits : c_auto;
     if (c < 2 || c > 24) return LZK_EINVAL;
@@ -250,7 +290,15 @@ int run_msm(const Fr* scalars, const Aff<typename Gp::F>* bases, size_t n, Jac<t
     uint32_t* large = reinterpret_cast<uint32_t*>(base + p.o_large);
     LZK_TRY(msm_sort(p, scalars, cnt, off, ent, bsums, st));
     void* tr = trace_begin(sizeof(F) == 32 ? "msm_g1_accumulate" : "msm_g2_accumulate", st);
-    k_accumulate<F><<<grid_for(p.chunks, 128), 128, 0, st>>>(bases, ent, off, p.B, p.chunks, bsum, head, tail); note_launch();
+    {
+        unsigned g = grid_for(p.chunks, 128);
+        constexpr int REF = sizeof(F) == 32 ? (int)LZK_BASES_REF_G1_JAC : (int)LZK_BASES_REF_G2_LANES;
+        if (layout == LZK_BASES_AFFINE) {
+            k_accumulate<F, LZK_BASES_AFFINE><<<g, 128, 0, st>>>(bases, ent, off, p.B, p.chunks, bsum, head, tail); note_launch();
+        } else {
+            k_accumulate<F, REF><<<g, 128, 0, st>>>(bases, ent, off, p.B, p.chunks, bsum, head, tail); note_launch();
+        }
+    }
     trace_end(tr, st);
     LZK_CUDA(cudaMemsetAsync(large, 0, sizeof(uint32_t), st));
     k_fixup<F><<<grid_for(p.B, 256, 148 * 8), 256, 0, st>>>(off, p.B, bsum, head, tail, large); note_launch();

@@ -6,11 +6,11 @@ using namespace lzk;
 
 extern "C" {
 
-int lzk_msm_g1(const lzk_fr_t* scalars, const lzk_g1_affine_t* bases, size_t n, lzk_g1_t* out,
+int lzk_msm_g1(const lzk_fr_t* scalars, const void* bases, size_t n, lzk_g1_t* out,
                const lzk_msm_cfg* cfg, void* stream)
 {
     bool shared = cfg && (cfg->flags & LZK_MSM_PRECOMPUTED);
-    return run_msm<G1>(reinterpret_cast<const Fr*>(scalars), reinterpret_cast<const Aff<Fq>*>(bases), n,
+    return run_msm<G1>(reinterpret_cast<const Fr*>(scalars), bases, n,
                        reinterpret_cast<Jac<Fq>*>(out), cfg, as_stream(stream), msm_autotune(1, n, shared));
 }
 

@@ -6,11 +6,11 @@ using namespace lzk;
 
 extern "C" {
 
-int lzk_msm_g2(const lzk_fr_t* scalars, const lzk_g2_affine_t* bases, size_t n, lzk_g2_t* out,
+int lzk_msm_g2(const lzk_fr_t* scalars, const void* bases, size_t n, lzk_g2_t* out,
                const lzk_msm_cfg* cfg, void* stream)
 {
     bool shared = cfg && (cfg->flags & LZK_MSM_PRECOMPUTED);
-    return run_msm<G2>(reinterpret_cast<const Fr*>(scalars), reinterpret_cast<const Aff<Fq2>*>(bases), n,
+    return run_msm<G2>(reinterpret_cast<const Fr*>(scalars), bases, n,
                        reinterpret_cast<Jac<Fq2>*>(out), cfg, as_stream(stream), msm_autotune(2, n, shared));
 }
 
