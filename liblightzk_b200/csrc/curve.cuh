@@ -66,6 +66,18 @@ __device__ __forceinline__ Fq2 csqr(const Fq2& a)
     Fq ab = mul_call(a.c0, a.c1);
     return {mul_call(add(a.c0, a.c1), sub(a.c0, a.c1)), dbl(ab)};
 }
+// two independent products: Fq pairs share one out-of-line body
+__device__ __forceinline__ void cmul2(Fq& r0, Fq& r1, const Fq& a0, const Fq& b0, const Fq& a1, const Fq& b1)
+{
+    FpPair<FqP> r = mul2_call(a0, b0, a1, b1);
+    r0 = r.a;
+    r1 = r.b;
+}
+__device__ __forceinline__ void cmul2(Fq2& r0, Fq2& r1, const Fq2& a0, const Fq2& b0, const Fq2& a1, const Fq2& b1)
+{
+    r0 = cmul(a0, b0);
+    r1 = cmul(a1, b1);
+}
 
 // ---------------- point forms ----------------
 template <class F> struct Aff { F x, y; };
@@ -96,63 +108,77 @@ template <class F> __device__ __forceinline__ XYZZ<F> xyzz_mdbl(const Aff<F>& a)
     return {X3, Y3, V, W};
 }
 
-// 2*P (dbl-2008-s-1)
+// 2*P (dbl-2008-s-1); independent products in pairs
 template <class F> __device__ __forceinline__ XYZZ<F> xyzz_dbl(const XYZZ<F>& p)
 {
     if (xyzz_is_inf(p)) return p;
     F U = dbl(p.Y);
-    F V = csqr(U);
-    F W = cmul(U, V);
-    F S = cmul(p.X, V);
-    F x2 = csqr(p.X);
+    F V, x2;
+    cmul2(V, x2, U, U, p.X, p.X);
+    F W, S;
+    cmul2(W, S, U, V, p.X, V);
     F M = add(dbl(x2), x2);
-    F X3 = sub(csqr(M), dbl(S));
-    F Y3 = sub(cmul(M, sub(S, X3)), cmul(W, p.Y));
-    return {X3, Y3, cmul(V, p.ZZ), cmul(W, p.ZZZ)};
+    F MM, ZZ3;
+    cmul2(MM, ZZ3, M, M, V, p.ZZ);
+    F X3 = sub(MM, dbl(S));
+    F t, u;
+    cmul2(t, u, M, sub(S, X3), W, p.Y);
+    F ZZZ3 = cmul(W, p.ZZZ);
+    return {X3, sub(t, u), ZZ3, ZZZ3};
 }
 
-// P + Q with Q affine (madd-2008-s); handles infinity, P == Q and P == -Q
+// P + Q with Q affine (madd-2008-s); handles infinity, P == Q and P == -Q.
+// Independent products are issued in pairs.
 template <class F> __device__ __forceinline__ XYZZ<F> xyzz_madd(const XYZZ<F>& p, const Aff<F>& q)
 {
     if (aff_is_inf(q)) return p;
     if (xyzz_is_inf(p)) return xyzz_from_aff(q);
-    F U2 = cmul(q.x, p.ZZ);
-    F S2 = cmul(q.y, p.ZZZ);
+    F U2, S2;
+    cmul2(U2, S2, q.x, p.ZZ, q.y, p.ZZZ);
     F P = sub(U2, p.X);
     F R = sub(S2, p.Y);
     if (P.is_zero()) {
         if (R.is_zero()) return xyzz_mdbl(q);
         return xyzz_inf<F>();
     }
-    F PP = csqr(P);
-    F PPP = cmul(P, PP);
-    F Q = cmul(p.X, PP);
-    F X3 = sub(sub(csqr(R), PPP), dbl(Q));
-    F Y3 = sub(cmul(R, sub(Q, X3)), cmul(p.Y, PPP));
-    return {X3, Y3, cmul(p.ZZ, PP), cmul(p.ZZZ, PPP)};
+    F PP, RR;
+    cmul2(PP, RR, P, P, R, R);
+    F PPP, Q;
+    cmul2(PPP, Q, P, PP, p.X, PP);
+    F X3 = sub(sub(RR, PPP), dbl(Q));
+    F t, ZZ3;
+    cmul2(t, ZZ3, R, sub(Q, X3), p.ZZ, PP);
+    F u, ZZZ3;
+    cmul2(u, ZZZ3, p.Y, PPP, p.ZZZ, PPP);
+    return {X3, sub(t, u), ZZ3, ZZZ3};
 }
 
-// P + Q (add-2008-s)
+// P + Q (add-2008-s); independent products in pairs
 template <class F> __device__ __forceinline__ XYZZ<F> xyzz_add(const XYZZ<F>& p, const XYZZ<F>& q)
 {
     if (xyzz_is_inf(q)) return p;
     if (xyzz_is_inf(p)) return q;
-    F U1 = cmul(p.X, q.ZZ);
-    F U2 = cmul(q.X, p.ZZ);
-    F S1 = cmul(p.Y, q.ZZZ);
-    F S2 = cmul(q.Y, p.ZZZ);
+    F U1, U2, S1, S2;
+    cmul2(U1, U2, p.X, q.ZZ, q.X, p.ZZ);
+    cmul2(S1, S2, p.Y, q.ZZZ, q.Y, p.ZZZ);
     F P = sub(U2, U1);
     F R = sub(S2, S1);
     if (P.is_zero()) {
         if (R.is_zero()) return xyzz_dbl(p);
         return xyzz_inf<F>();
     }
-    F PP = csqr(P);
-    F PPP = cmul(P, PP);
-    F Q = cmul(U1, PP);
-    F X3 = sub(sub(csqr(R), PPP), dbl(Q));
-    F Y3 = sub(cmul(R, sub(Q, X3)), cmul(S1, PPP));
-    return {X3, Y3, cmul(cmul(p.ZZ, q.ZZ), PP), cmul(cmul(p.ZZZ, q.ZZZ), PPP)};
+    F PP, RR;
+    cmul2(PP, RR, P, P, R, R);
+    F PPP, Q;
+    cmul2(PPP, Q, P, PP, U1, PP);
+    F X3 = sub(sub(RR, PPP), dbl(Q));
+    F t, u;
+    cmul2(t, u, R, sub(Q, X3), S1, PPP);
+    F zz, zzz;
+    cmul2(zz, zzz, p.ZZ, q.ZZ, p.ZZZ, q.ZZZ);
+    F ZZ3, ZZZ3;
+    cmul2(ZZ3, ZZZ3, zz, PP, zzz, PPP);
+    return {X3, sub(t, u), ZZ3, ZZZ3};
 }
 
 template <class F> __device__ __forceinline__ XYZZ<F> xyzz_neg(const XYZZ<F>& p) { return {p.X, neg(p.Y), p.ZZ, p.ZZZ}; }

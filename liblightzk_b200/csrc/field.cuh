@@ -244,6 +244,18 @@ template <class P> __device__ __forceinline__ Fp<P> sqr(const Fp<P>& a) { return
 // additions (ten products each) would not fit.
 template <class P> __device__ __noinline__ Fp<P> mul_call(const Fp<P> a, const Fp<P> b) { return mul(a, b); }
 
+// Two independent products in one out-of-line body, so their carry chains
+// can be interleaved (instruction-level parallelism 2 per thread).
+template <class P>
+struct FpPair {
+    Fp<P> a, b;
+};
+template <class P>
+__device__ __noinline__ FpPair<P> mul2_call(const Fp<P> a0, const Fp<P> b0, const Fp<P> a1, const Fp<P> b1)
+{
+    return FpPair<P>{mul(a0, b0), mul(a1, b1)};
+}
+
 // Montgomery -> canonical integer (multiply by 1)
 template <class P>
 __device__ __forceinline__ Fp<P> from_mont(const Fp<P>& a)

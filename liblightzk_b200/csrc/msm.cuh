@@ -10,7 +10,7 @@ struct G1 { using F = Fq; };
 struct G2 { using F = Fq2; };
 
 constexpr uint32_t kAccChunk = 32;   // sorted entries per accumulation thread
-constexpr uint32_t kLevelL = 8;      // buckets per thread in a reduction level
+constexpr uint32_t kLevelL = 32;     // buckets per warp in a reduction level
 constexpr uint32_t kFixSmall = 64;   // partials a single fix-up thread folds
 
 struct MsmPlan {
@@ -40,7 +40,9 @@ inline void plan_msm(MsmPlan& p, size_t n, uint32_t c, bool shared, size_t strid
     p.B = p.wb * p.nb;
     p.max_entries = n * (size_t)p.W;
     p.chunks = (p.max_entries + kAccChunk - 1) / kAccChunk;
-    size_t lvl = (p.B + kLevelL - 1) / kLevelL;
+    // the first reduction level writes wb * max(1, nb / kLevelL) points; later
+    // levels write fewer
+    size_t lvl = (size_t)p.wb * (p.nb > kLevelL ? p.nb / kLevelL : 1);
     Carver cv;
     p.o_cnt = cv.take<uint32_t>(p.B);
     p.o_off = cv.take<uint32_t>(p.B + 1);
@@ -198,32 +200,79 @@ __global__ void k_fixup_large(const uint32_t* __restrict__ off, XYZZ<F>* __restr
     }
 }
 
-// One level of the weighted bucket sum.  Per window, the input holds m
-// points X_k; thread (w, s) covers X_{sL..sL+L-1} and writes
-//   R_s = sum_j X_{sL+j}
-//   A_s = sum_j Ain_{sL+j} + 2^logM * sum_j (j + base) X_{sL+j}
-// so that sum_k (k + base) X_k = sum_s t_s + L * sum_s s R_s at every level.
+// Warp shuffles of whole points
 template <class F>
-__global__ void k_level(const XYZZ<F>* __restrict__ inR, const XYZZ<F>* __restrict__ inA,
-                        const uint32_t* __restrict__ off, uint32_t windows, uint32_t m, uint32_t L,
-                        uint32_t base, uint32_t logM, XYZZ<F>* __restrict__ outR, XYZZ<F>* __restrict__ outA)
+__device__ __forceinline__ XYZZ<F> shfl_down_pt(const XYZZ<F>& x, uint32_t d)
 {
-    uint32_t segs = m / L;
-    uint64_t total = (uint64_t)windows * segs;
-    for (uint64_t t = gtid(); t < total; t += gstride()) {
-        uint32_t w = (uint32_t)(t / segs), s = (uint32_t)(t % segs);
+    XYZZ<F> r;
+    const uint32_t* s = reinterpret_cast<const uint32_t*>(&x);
+    uint32_t* o = reinterpret_cast<uint32_t*>(&r);
+    _Pragma("unroll") for (int i = 0; i < (int)(sizeof(XYZZ<F>) / 4); i++) o[i] = __shfl_down_sync(0xffffffffu, s[i], d);
+    return r;
+}
+template <class F>
+__device__ __forceinline__ XYZZ<F> shfl_xor_pt(const XYZZ<F>& x, uint32_t m)
+{
+    XYZZ<F> r;
+    const uint32_t* s = reinterpret_cast<const uint32_t*>(&x);
+    uint32_t* o = reinterpret_cast<uint32_t*>(&r);
+    _Pragma("unroll") for (int i = 0; i < (int)(sizeof(XYZZ<F>) / 4); i++) o[i] = __shfl_xor_sync(0xffffffffu, s[i], m);
+    return r;
+}
+template <class F>
+__device__ __forceinline__ XYZZ<F> shfl_pt(const XYZZ<F>& x, uint32_t lane)
+{
+    XYZZ<F> r;
+    const uint32_t* s = reinterpret_cast<const uint32_t*>(&x);
+    uint32_t* o = reinterpret_cast<uint32_t*>(&r);
+    _Pragma("unroll") for (int i = 0; i < (int)(sizeof(XYZZ<F>) / 4); i++) o[i] = __shfl_sync(0xffffffffu, s[i], lane);
+    return r;
+}
+
+// One level of the weighted bucket sum, one warp per segment of L <= 32
+// consecutive points.  Per window the input holds m points X_k; for the
+// segment s, lane j holds X_{sL+j}, a shuffle scan forms the suffix sums
+// S_j = sum_{k >= j} X_{sL+k}, and
+//   R_s = S_0,
+//   t_s = sum_{j >= 1 - base} S_j = sum_j (j + base) X_{sL+j},
+//   A_s = sum_j Ain_{sL+j} + 2^logM * t_s,
+// so that sum_k (k + base) X_k = sum_s t_s + L * sum_s s R_s: the next level
+// (base 0) reduces the R_s, and the A's carry the weighted partial results
+// (scaled by the product of the earlier segment lengths) to the top.  Empty
+// buckets (off[k] == off[k+1]) read as the point at infinity.
+template <class F>
+__global__ void __launch_bounds__(128) k_level(const XYZZ<F>* __restrict__ inR, const XYZZ<F>* __restrict__ inA,
+                                               const uint32_t* __restrict__ off, uint32_t windows, uint32_t m,
+                                               uint32_t L, uint32_t base, uint32_t logM, XYZZ<F>* __restrict__ outR,
+                                               XYZZ<F>* __restrict__ outA)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t segs = m / L;
+    const uint64_t total = (uint64_t)windows * segs;
+    for (uint64_t seg = gtid() >> 5; seg < total; seg += gstride() >> 5) {
+        uint32_t w = (uint32_t)(seg / segs), s = (uint32_t)(seg % segs);
         size_t first = (size_t)w * m + (size_t)s * L;
-        XYZZ<F> run = xyzz_inf<F>(), acc = xyzz_inf<F>(), A = xyzz_inf<F>();
-        for (int j = (int)L - 1; j >= 0; j--) {
-            size_t k = first + j;
-            XYZZ<F> x = (off && off[k] == off[k + 1]) ? xyzz_inf<F>() : ld_elem(inR + k);
-            run = xyzz_add_cold(run, x);
-            if (j > 0 || base) acc = xyzz_add_cold(acc, run);
-            if (inA) A = xyzz_add_cold(A, ld_elem(inA + k));
+        XYZZ<F> S = xyzz_inf<F>(), A = xyzz_inf<F>();
+        if (lane < L) {
+            size_t k = first + lane;
+            if (!off || off[k] != off[k + 1]) S = ld_elem(inR + k);
+            if (inA) A = ld_elem(inA + k);
         }
-        for (uint32_t d = 0; d < logM; d++) acc = xyzz_dbl_cold(acc);
-        st_elem(outR + t, run);
-        st_elem(outA + t, xyzz_add_cold(A, acc));
+        for (uint32_t d = 1; d < L; d <<= 1) {
+            XYZZ<F> o = shfl_down_pt(S, d);
+            if (lane + d < L) S = xyzz_add_cold(S, o);
+        }
+        XYZZ<F> R = shfl_pt(S, 0);
+        XYZZ<F> t = (lane < L && (lane >= 1 || base)) ? S : xyzz_inf<F>();
+        for (uint32_t d = 16; d > 0; d >>= 1) {
+            t = xyzz_add_cold(t, shfl_xor_pt(t, d));
+            if (inA) A = xyzz_add_cold(A, shfl_xor_pt(A, d));
+        }
+        if (lane == 0) {
+            for (uint32_t d = 0; d < logM; d++) t = xyzz_dbl_cold(t);
+            st_elem(outR + seg, R);
+            st_elem(outA + seg, xyzz_add_cold(A, t));
+        }
     }
 }
 
@@ -315,7 +364,7 @@ int run_msm(const Fr* scalars, const void* bases, size_t n, Jac<typename Gp::F>*
     while (true) {
         uint32_t L = m < kLevelL ? m : kLevelL;
         uint32_t segs = m / L;
-        size_t threads = (size_t)p.wb * segs;
+        size_t threads = (size_t)p.wb * segs * 32;
         k_level<F><<<grid_for(threads, 128), 128, 0, st>>>(inR, inA, offp, p.wb, m, L, base1, logM, lr[pp], la[pp]); note_launch();
         inR = lr[pp]; inA = la[pp]; resA = la[pp];
         offp = nullptr; base1 = 0;
