@@ -107,6 +107,27 @@ size_t lzk_msm_workspace_bytes(int group, size_t n, const lzk_msm_cfg* cfg);
  * precomputed or not). */
 uint32_t lzk_msm_autotune_window(int group, size_t n, uint32_t flags);
 
+/* G1 MSM over plain affine bases that allocates no device memory, for
+ * callers that cannot let a library allocate: processes that give all device
+ * memory to their own allocator at start-up, and latency-bound request paths
+ * that must not wait on the allocator or run out of memory mid-request.  No
+ * counterpart in the reference (its MSM allocates scratch on every call,
+ * msm.cuh:216-219, with no alternative).
+ *
+ * Scratch is a fixed LZK_MSM_NOALLOC_SCRATCH_BYTES array in device memory
+ * that the library reserves on every GPU that loads it, for the life of the
+ * process.  n may be at most LZK_MSM_NOALLOC_MAX_POINTS, and the scratch of
+ * the chosen window (window_bits, 0 = autotuned) must fit; otherwise the call
+ * returns LZK_EINVAL without queuing work.  The first call on each device
+ * looks up the array's device address (cudaGetSymbolAddress), so make it
+ * before beginning any stream capture.  All calls on a device share the
+ * array: the counters that must start at zero are cleared by every call, but
+ * calls whose work overlaps on the GPU race -- order them. */
+#define LZK_MSM_NOALLOC_MAX_POINTS   65536u
+#define LZK_MSM_NOALLOC_SCRATCH_BYTES (32u << 20)
+int lzk_msm_g1_noalloc(const lzk_fr_t* scalars, const lzk_g1_affine_t* bases, size_t n, lzk_g1_t* out,
+                       uint32_t window_bits, void* stream);
+
 /* Build the shifted-copy table for LZK_MSM_PRECOMPUTED: table[j*level_stride
  * + i] = 2^(j*window_bits) * bases[i], affine, j < windows.  Replaces
  * pre_comp_g1/_g2 (msm.cuh:48-75).  level_stride >= n. */

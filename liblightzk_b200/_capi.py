@@ -20,6 +20,7 @@ SIGNATURES = {
     "lzk_version": (ctypes.c_char_p, []),
     "lzk_msm_g1": (c_i, [c_p, c_p, c_sz, c_p, c_p, c_p]),
     "lzk_msm_g2": (c_i, [c_p, c_p, c_sz, c_p, c_p, c_p]),
+    "lzk_msm_g1_noalloc": (c_i, [c_p, c_p, c_sz, c_p, c_u32, c_p]),
     "lzk_msm_workspace_bytes": (c_sz, [c_i, c_sz, c_p]),
     "lzk_msm_autotune_window": (c_u32, [c_i, c_sz, c_u32]),
     "lzk_g1_precompute": (c_i, [c_p, c_sz, c_u32, c_u32, c_p, c_sz, c_p]),
