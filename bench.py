@@ -43,7 +43,7 @@ def parse():
     ap.add_argument("--mode", choices=["standard", "reference"], default="standard")
     ap.add_argument("--window", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", choices=["prove", "msm-g1", "msm-g2", "ntt"], default="prove",
+    ap.add_argument("--case", choices=["prove", "msm-g1", "msm-g2", "ntt", "batch"], default="prove",
                     help="prove = the benchmark; the others run one operator at --log-n for profiling")
     ap.add_argument("--log-n", type=int, default=20)
     ap.add_argument("--reps", type=int, default=3)
@@ -180,11 +180,58 @@ def run_reference_arm(args, rank, world):
 
 
 # --------------------------------------------------------------- GPU side
+def run_batch_case(args):
+    """the batched-operator workload (64 G1 MSMs of 2^10..2^20 points and 32
+    NTTs of 2^12..2^22 elements): one batch plan replayed as a CUDA graph,
+    against the same operators called one at a time"""
+    import torch
+
+    from liblightzk_b200 import autotune, batch, msm, ntt
+    tuned = autotune.tune(1, log_ns=range(10, 21), spread=2, reps=2)
+    msms, ntts, _pool = batch.workload_config3()
+    plan = batch.BatchPlan(1, msms, ntts)
+    stream = torch.cuda.Stream()
+    torch.cuda.synchronize()
+
+    def timed(fn, reps):
+        out = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            torch.cuda.synchronize()
+            out.append(a.elapsed_time(b))
+        return out
+
+    plan.run(use_graph=True, stream=stream)
+    torch.cuda.synchronize()
+    plan_ms = timed(lambda: plan.run(use_graph=True, stream=stream), args.reps)
+
+    def one_by_one():
+        for s, b, o in msms:
+            msm.msm(1, s, b, out=o, stream=stream)
+        for d, k, di in ntts:
+            ntt.ntt(d, k, di, stream=stream)
+
+    one_by_one()
+    seq_ms = timed(one_by_one, args.reps)
+    pts = sum(int(m[0].shape[0]) for m in msms)
+    elems = sum(1 << k for _, k, _ in ntts)
+    print(json.dumps({"case": "batch", "msms": len(msms), "ntts": len(ntts), "msm_points": pts,
+                      "ntt_elements": elems, "plan_graph_ms": plan_ms, "one_by_one_ms": seq_ms,
+                      "speedup": float(np.median(seq_ms) / np.median(plan_ms)),
+                      "plan_device_bytes": plan.device_bytes(),
+                      "tuned_windows": {lg: v[0] for lg, v in tuned.items()}}), flush=True)
+
+
 def run_case(args):
     """one operator at 2^log_n, `reps` times, for profiling (prints ms)"""
     import torch
 
     from liblightzk_b200 import msm, ntt, synth
+    if args.case == "batch":
+        return run_batch_case(args)
     n = 1 << args.log_n
     sc = synth.random_fr(n, 5, 77)
     out = []

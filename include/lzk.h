@@ -268,6 +268,46 @@ size_t lzk_prover_device_bytes(const lzk_prover* prover);
 int lzk_groth16_prove(lzk_prover* prover, const lzk_fr_t* z, const lzk_fr_t* r, const lzk_fr_t* s,
                       lzk_groth16_proof* proof, void* stream);
 
+/* ------------------------------------------------------------ batching
+ * Many MSMs (one group: 1 = G1, 2 = G2; plain affine bases) and NTTs of
+ * uneven sizes as one plan.  All MSMs share one global bucket space, so each
+ * MSM phase is a single launch for the whole batch; NTTs are grouped by
+ * (size, direction) on a second stream.  The plan allocates everything when
+ * it is created, so running it is launches only; with use_graph the plan
+ * captures those launches into a CUDA graph on the first run (stream must
+ * then be a created stream, not the legacy default) and replays it after.
+ * The descriptors' buffers must stay valid while the plan lives; their
+ * contents may change between runs.  Extends the reference's one-call-per-
+ * operator interface (msm.cuh:210-247, poly.cuh:65-73). */
+typedef struct lzk_msm_desc {
+    const lzk_fr_t* scalars;   /* device, n Fr (Montgomery) */
+    const void* bases;         /* device, n affine points */
+    size_t n;
+    void* out;                 /* device, one Jacobian point */
+    uint32_t window_bits;      /* 0 = autotuned */
+    uint32_t reserved;
+} lzk_msm_desc;
+
+typedef struct lzk_ntt_desc {
+    lzk_fr_t* data;            /* device, 2^log_n Fr, transformed in place */
+    uint32_t log_n;
+    int direction;             /* LZK_NTT_* */
+} lzk_ntt_desc;
+
+typedef struct lzk_batch_plan lzk_batch_plan;
+
+int lzk_batch_plan_create(int group, const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_desc* ntts, size_t n_ntt,
+                          lzk_batch_plan** out);
+int lzk_batch_plan_run(lzk_batch_plan* plan, int use_graph, void* stream);
+size_t lzk_batch_plan_device_bytes(const lzk_batch_plan* plan);
+int lzk_batch_plan_destroy(lzk_batch_plan* plan);
+
+/* Autotuner table: the window width plain-base MSMs of about 2^log_n points
+ * use when their cfg asks for autotuning (window_bits = 0 clears the entry
+ * and falls back to the cost model).  Filled from timings by
+ * liblightzk_b200.autotune. */
+int lzk_msm_set_window(int group, uint32_t log_n, uint32_t window_bits);
+
 /* ------------------------------------------------------------ tracing
  * Opt-in CUDA-event timing of named device regions ("msm_g1",
  * "msm_g1_accumulate", "msm_g2", "msm_g2_accumulate", "groth16_prove").

@@ -44,6 +44,11 @@ SIGNATURES = {
     "lzk_prover_destroy": (c_i, [c_p]),
     "lzk_prover_device_bytes": (c_sz, [c_p]),
     "lzk_groth16_prove": (c_i, [c_p, c_p, c_p, c_p, c_p, c_p]),
+    "lzk_batch_plan_create": (c_i, [c_i, c_p, c_sz, c_p, c_sz, c_p]),
+    "lzk_batch_plan_run": (c_i, [c_p, c_i, c_p]),
+    "lzk_batch_plan_device_bytes": (c_sz, [c_p]),
+    "lzk_batch_plan_destroy": (c_i, [c_p]),
+    "lzk_msm_set_window": (c_i, [c_i, c_u32, c_u32]),
     "lzk_trace_enable": (None, [c_i]),
     "lzk_trace_reset": (None, []),
     "lzk_trace_get": (c_i, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64)]),
@@ -84,6 +89,19 @@ class Csr(ctypes.Structure):
         ("index_bytes", ctypes.c_uint32),
         ("reserved", ctypes.c_uint32),
     ]
+
+
+class MsmDesc(ctypes.Structure):
+    """struct lzk_msm_desc"""
+
+    _fields_ = [("scalars", ctypes.c_void_p), ("bases", ctypes.c_void_p), ("n", ctypes.c_size_t),
+                ("out", ctypes.c_void_p), ("window_bits", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class NttDesc(ctypes.Structure):
+    """struct lzk_ntt_desc"""
+
+    _fields_ = [("data", ctypes.c_void_p), ("log_n", ctypes.c_uint32), ("direction", ctypes.c_int)]
 
 
 class LzkError(RuntimeError):

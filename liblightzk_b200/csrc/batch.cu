@@ -1,0 +1,369 @@
+// batch.cu -- many MSMs and NTTs of uneven sizes as one plan.
+//
+// The reference runs one operator per call, each with its own allocations
+// and launches (msm.cuh:210-247, poly.cuh:65-73).  A batch plan lays every
+// MSM of the batch into one global bucket space and runs each MSM phase
+// once for the whole batch:
+//   gather bases -> digit count -> offset scan -> scatter -> accumulate
+//   -> fix-up -> bucket reduction (one level chain per window width) ->
+//   window combination (one thread per MSM)
+// so 64 MSMs cost about the launches of one.  MSMs are ordered by window
+// width so that the windows of equal width are contiguous and reduce
+// together.  NTTs are grouped by (size, direction) and each group is one
+// set of pass launches over a device table of pointers, on a second stream
+// that overlaps the MSM phases.  Every buffer is allocated when the plan is
+// made, so running a plan is launches only; the plan captures them into a
+// CUDA graph on first use and replays the graph afterwards.
+#include "msm.cuh"
+#include "ntt.cuh"
+#include <algorithm>
+#include <map>
+#include <vector>
+
+struct BDesc {                 // per MSM, device side
+    const lzk::Fr* scalars;
+    const void* bases;
+    uint64_t pts_off;          // first point in the gathered base array
+    uint64_t n;
+    uint64_t bucket_base;      // first bucket in the global bucket space
+    uint64_t win_base;         // first window in the window-result array
+    void* out;
+    uint32_t c, W, nb, pad;
+};
+
+struct lzk_batch_plan {
+    int group = 1;
+    std::vector<BDesc> msm;            // sorted by window width
+    struct WGroup { uint32_t c; uint64_t bucket_base, windows; };
+    std::vector<WGroup> wgroups;
+    struct NGroup { uint32_t k; int dir; uint32_t count; lzk::Fr** ptrs; };
+    std::vector<NGroup> ngroups;
+    uint64_t total_pts = 0, total_buckets = 0, total_windows = 0, max_entries = 0, chunks = 0, lvl = 0;
+    char* ws = nullptr;
+    size_t ws_bytes = 0;
+    BDesc* d_desc = nullptr;
+    uint64_t* d_ptsoff = nullptr;
+    uint32_t *cnt = nullptr, *off = nullptr, *ent = nullptr, *bsums = nullptr, *large = nullptr;
+    void *bases = nullptr, *bsum = nullptr, *head = nullptr, *tail = nullptr, *lr[2] = {nullptr, nullptr},
+         *la[2] = {nullptr, nullptr}, *wres = nullptr;
+    cudaStream_t s_ntt = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t graph_stream = nullptr;
+};
+
+namespace lzk {
+
+__device__ __forceinline__ uint32_t find_msm(const uint64_t* ptsoff, uint32_t count, uint64_t i)
+{
+    uint32_t lo = 0, hi = count;   // largest k with ptsoff[k] <= i
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (ptsoff[mid] <= i) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+template <class F>
+__global__ void k_bgather(const BDesc* __restrict__ d, const uint64_t* __restrict__ ptsoff, uint32_t count,
+                          uint64_t total, Aff<F>* __restrict__ dst)
+{
+    for (uint64_t i = gtid(); i < total; i += gstride()) {
+        uint32_t k = find_msm(ptsoff, count, i);
+        st_elem(dst + i, ldg_elem(reinterpret_cast<const Aff<F>*>(d[k].bases) + (i - d[k].pts_off)));
+    }
+}
+
+// signed digits of every scalar of the batch (the recoding of msm_sort.cu)
+__device__ __forceinline__ uint32_t bwindow_bits(const uint32_t s[8], uint32_t lo, uint32_t c)
+{
+    uint32_t w = lo >> 5, sh = lo & 31;
+    if (w >= 8) return 0;
+    uint64_t v = ((uint64_t)s[w] | ((uint64_t)(w + 1 < 8 ? s[w + 1] : 0u) << 32)) >> sh;
+    return (uint32_t)v & ((1u << c) - 1u);
+}
+
+template <bool SCATTER>
+__global__ void k_bdigits(const BDesc* __restrict__ d, const uint64_t* __restrict__ ptsoff, uint32_t count,
+                          uint64_t total, const uint32_t* __restrict__ off, uint32_t* __restrict__ cnt,
+                          uint32_t* __restrict__ ent)
+{
+    for (uint64_t i = gtid(); i < total; i += gstride()) {
+        uint32_t k = find_msm(ptsoff, count, i);
+        const BDesc& m = d[k];
+        Fr sc = from_mont(ldg_elem(m.scalars + (i - m.pts_off)));
+        uint32_t carry = 0, half = m.nb;
+        for (uint32_t w = 0; w < m.W; w++) {
+            uint32_t raw = bwindow_bits(sc.v, w * m.c, m.c) + carry;
+            uint32_t a;
+            bool neg;
+            if (raw > half) { carry = 1; neg = true; a = (1u << m.c) - raw; }
+            else { carry = 0; neg = false; a = raw; }
+            if (!a) continue;
+            uint32_t b = (uint32_t)(m.bucket_base + (uint64_t)w * m.nb + a - 1);
+            if (SCATTER) {
+                uint32_t slot = off[b] + atomicSub(cnt + b, 1u) - 1u;
+                ent[slot] = (uint32_t)i | (neg ? 0x80000000u : 0u);
+            } else {
+                atomicAdd(cnt + b, 1u);
+            }
+        }
+    }
+}
+
+// Horner over each MSM's windows, one thread per MSM
+template <class F>
+__global__ void k_bfinish(const BDesc* __restrict__ d, uint32_t count, const XYZZ<F>* __restrict__ wres)
+{
+    for (uint64_t k = gtid(); k < count; k += gstride()) {
+        const BDesc& m = d[k];
+        XYZZ<F> r = xyzz_inf<F>();
+        for (int w = (int)m.W - 1; w >= 0; w--) {
+            if (w != (int)m.W - 1)
+                for (uint32_t b = 0; b < m.c; b++) r = xyzz_dbl_cold(r);
+            r = xyzz_add_cold(r, ld_elem(wres + m.win_base + w));
+        }
+        if (m.n == 0) r = xyzz_inf<F>();
+        st_elem(reinterpret_cast<Jac<F>*>(m.out), xyzz_to_jac(r));
+    }
+}
+
+template <class F>
+static int run_plan(lzk_batch_plan* p, cudaStream_t st)
+{
+    using X = XYZZ<F>;
+    uint32_t count = (uint32_t)p->msm.size();
+    if (count && p->total_pts) {
+        unsigned g = grid_for(p->total_pts, 256, 148 * 16);
+        k_bgather<F><<<g, 256, 0, st>>>(p->d_desc, p->d_ptsoff, count, p->total_pts, static_cast<Aff<F>*>(p->bases)); note_launch();
+        LZK_CUDA(cudaMemsetAsync(p->cnt, 0, sizeof(uint32_t) * p->total_buckets, st));
+        k_bdigits<false><<<g, 256, 0, st>>>(p->d_desc, p->d_ptsoff, count, p->total_pts, p->off, p->cnt, p->ent); note_launch();
+        LZK_TRY(scan_offsets(p->cnt, (uint32_t)p->total_buckets, p->off, p->bsums, st));
+        k_bdigits<true><<<g, 256, 0, st>>>(p->d_desc, p->d_ptsoff, count, p->total_pts, p->off, p->cnt, p->ent); note_launch();
+        X* bsum = static_cast<X*>(p->bsum);
+        k_accumulate<F, LZK_BASES_AFFINE><<<grid_for(p->chunks, 128), 128, 0, st>>>(
+            p->bases, p->ent, p->off, (uint32_t)p->total_buckets, p->chunks, bsum, static_cast<X*>(p->head),
+            static_cast<X*>(p->tail)); note_launch();
+        LZK_CUDA(cudaMemsetAsync(p->large, 0, sizeof(uint32_t), st));
+        k_fixup<F><<<grid_for(p->total_buckets, 256, 148 * 8), 256, 0, st>>>(p->off, (uint32_t)p->total_buckets, bsum,
+                                                                            static_cast<X*>(p->head),
+                                                                            static_cast<X*>(p->tail), p->large); note_launch();
+        constexpr unsigned fx_threads = 32768 / sizeof(X);
+        k_fixup_large<F><<<148 * 2, fx_threads, fx_threads * sizeof(X), st>>>(p->off, bsum, static_cast<X*>(p->head),
+                                                                             static_cast<X*>(p->tail), p->large); note_launch();
+        // one reduction chain per window width
+        uint64_t wdone = 0;
+        for (auto& wg : p->wgroups) {
+            const X* inR = bsum + wg.bucket_base;
+            const X* inA = nullptr;
+            const uint32_t* offp = p->off + wg.bucket_base;
+            uint32_t m = 1u << (wg.c - 1), logM = 0, base1 = 1, pp = 0;
+            while (true) {
+                uint32_t L = m < kLevelL ? m : kLevelL;
+                uint32_t segs = m / L;
+                bool last = segs == 1;
+                X* outR = static_cast<X*>(p->lr[pp]);
+                X* outA = last ? static_cast<X*>(p->wres) + wdone : static_cast<X*>(p->la[pp]);
+                size_t threads = (size_t)wg.windows * segs * 32;
+                k_level<F><<<grid_for(threads, 128), 128, 0, st>>>(inR, inA, offp, (uint32_t)wg.windows, m, L, base1, logM,
+                                                                  outR, outA); note_launch();
+                inR = outR; inA = outA; offp = nullptr; base1 = 0;
+                uint32_t lg = 0; while ((1u << lg) < L) lg++;
+                logM += lg;
+                m = segs;
+                pp ^= 1;
+                if (last) break;
+            }
+            wdone += wg.windows;
+        }
+        k_bfinish<F><<<grid_for(count, 32), 32, 0, st>>>(p->d_desc, count, static_cast<const X*>(p->wres)); note_launch();
+    } else if (count) {
+        k_bfinish<F><<<grid_for(count, 32), 32, 0, st>>>(p->d_desc, count, static_cast<const X*>(p->wres)); note_launch();
+    }
+    return launch_status();
+}
+
+static int run_all(lzk_batch_plan* p, cudaStream_t st)
+{
+    if (!p->ngroups.empty()) {
+        LZK_CUDA(cudaEventRecord(p->ev_fork, st));
+        LZK_CUDA(cudaStreamWaitEvent(p->s_ntt, p->ev_fork, 0));
+        for (auto& g : p->ngroups) LZK_TRY(ntt_run(nullptr, g.k, g.dir, g.count, 0, nullptr, p->s_ntt, g.ptrs));
+        LZK_CUDA(cudaEventRecord(p->ev_join, p->s_ntt));
+    }
+    LZK_TRY(p->group == 2 ? run_plan<Fq2>(p, st) : run_plan<Fq>(p, st));
+    if (!p->ngroups.empty()) LZK_CUDA(cudaStreamWaitEvent(st, p->ev_join, 0));
+    return LZK_OK;
+}
+
+static void destroy_plan(lzk_batch_plan* p)
+{
+    if (!p) return;
+    if (p->exec) cudaGraphExecDestroy(p->exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    if (p->ws) cudaFree(p->ws);
+    for (auto& g : p->ngroups) if (g.ptrs) cudaFree(g.ptrs);
+    if (p->s_ntt) cudaStreamDestroy(p->s_ntt);
+    if (p->ev_fork) cudaEventDestroy(p->ev_fork);
+    if (p->ev_join) cudaEventDestroy(p->ev_join);
+    delete p;
+}
+
+template <class F>
+static int create_plan(const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_desc* ntts, size_t n_ntt,
+                       lzk_batch_plan* p)
+{
+    using X = XYZZ<F>;
+    // MSMs: widths, ordering, global layout
+    std::vector<size_t> order(n_msm);
+    std::vector<uint32_t> cw(n_msm);
+    for (size_t i = 0; i < n_msm; i++) {
+        if (!msms[i].out || (msms[i].n && (!msms[i].scalars || !msms[i].bases))) return LZK_EINVAL;
+        cw[i] = msms[i].window_bits ? msms[i].window_bits : msm_autotune(p->group, msms[i].n, false);
+        if (cw[i] < 2 || cw[i] > 24) return LZK_EINVAL;
+        order[i] = i;
+    }
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return cw[a] < cw[b]; });
+    std::vector<uint64_t> ptsoff;
+    for (size_t o : order) {
+        const lzk_msm_desc& m = msms[o];
+        BDesc d{};
+        d.scalars = reinterpret_cast<const Fr*>(m.scalars);
+        d.bases = m.bases;
+        d.n = m.n;
+        d.out = m.out;
+        d.c = cw[o];
+        d.W = windows_for(d.c);
+        d.nb = 1u << (d.c - 1);
+        d.pts_off = p->total_pts;
+        d.bucket_base = p->total_buckets;
+        d.win_base = p->total_windows;
+        p->total_pts += m.n;
+        p->total_buckets += (uint64_t)d.W * d.nb;
+        p->total_windows += d.W;
+        p->max_entries += m.n * (uint64_t)d.W;
+        if (p->wgroups.empty() || p->wgroups.back().c != d.c) p->wgroups.push_back({d.c, d.bucket_base, 0});
+        p->wgroups.back().windows += d.W;
+        ptsoff.push_back(d.pts_off);
+        p->msm.push_back(d);
+    }
+    if (p->total_pts >= (1ull << 31) || p->total_buckets >= (1ull << 32) - 1 || p->max_entries >= (1ull << 32))
+        return LZK_EINVAL;
+    p->chunks = (p->max_entries + kAccChunk - 1) / kAccChunk;
+    for (auto& g : p->wgroups) {
+        uint64_t nb = 1ull << (g.c - 1);
+        p->lvl = std::max<uint64_t>(p->lvl, g.windows * (nb > kLevelL ? nb / kLevelL : 1));
+    }
+    uint64_t B = std::max<uint64_t>(p->total_buckets, 1);
+    Carver cv;
+    size_t o_desc = cv.take<BDesc>(std::max<size_t>(n_msm, 1));
+    size_t o_ptsoff = cv.take<uint64_t>(std::max<size_t>(n_msm, 1));
+    size_t o_cnt = cv.take<uint32_t>(B), o_off = cv.take<uint32_t>(B + 1);
+    size_t o_bsums = cv.take<uint32_t>((B + 4095) / 4096 + 1);
+    size_t o_large = cv.take<uint32_t>(p->chunks / kFixSmall + 2);
+    size_t o_ent = cv.take<uint32_t>(std::max<uint64_t>(p->max_entries, 1));
+    size_t o_bases = cv.take<Aff<F>>(std::max<uint64_t>(p->total_pts, 1));
+    size_t o_bsum = cv.take<X>(B);
+    size_t o_head = cv.take<X>(std::max<uint64_t>(p->chunks, 1)), o_tail = cv.take<X>(std::max<uint64_t>(p->chunks, 1));
+    size_t o_lr0 = cv.take<X>(std::max<uint64_t>(p->lvl, 1)), o_lr1 = cv.take<X>(std::max<uint64_t>(p->lvl, 1));
+    size_t o_la0 = cv.take<X>(std::max<uint64_t>(p->lvl, 1)), o_la1 = cv.take<X>(std::max<uint64_t>(p->lvl, 1));
+    size_t o_wres = cv.take<X>(std::max<uint64_t>(p->total_windows, 1));
+    p->ws_bytes = cv.off;
+    if (cudaMalloc(&p->ws, p->ws_bytes) != cudaSuccess) { cudaGetLastError(); return LZK_ENOMEM; }
+    char* b = p->ws;
+    p->d_desc = reinterpret_cast<BDesc*>(b + o_desc);
+    p->d_ptsoff = reinterpret_cast<uint64_t*>(b + o_ptsoff);
+    p->cnt = reinterpret_cast<uint32_t*>(b + o_cnt);
+    p->off = reinterpret_cast<uint32_t*>(b + o_off);
+    p->bsums = reinterpret_cast<uint32_t*>(b + o_bsums);
+    p->large = reinterpret_cast<uint32_t*>(b + o_large);
+    p->ent = reinterpret_cast<uint32_t*>(b + o_ent);
+    p->bases = b + o_bases;
+    p->bsum = b + o_bsum;
+    p->head = b + o_head;
+    p->tail = b + o_tail;
+    p->lr[0] = b + o_lr0; p->lr[1] = b + o_lr1; p->la[0] = b + o_la0; p->la[1] = b + o_la1;
+    p->wres = b + o_wres;
+    if (n_msm) {
+        LZK_CUDA(cudaMemcpy(p->d_desc, p->msm.data(), sizeof(BDesc) * n_msm, cudaMemcpyHostToDevice));
+        LZK_CUDA(cudaMemcpy(p->d_ptsoff, ptsoff.data(), sizeof(uint64_t) * n_msm, cudaMemcpyHostToDevice));
+    }
+    // NTTs: groups of equal (size, direction) with a device pointer table each
+    std::map<std::pair<uint32_t, int>, std::vector<Fr*>> groups;
+    for (size_t i = 0; i < n_ntt; i++) {
+        if (!ntts[i].data || ntts[i].log_n > 26 || ntts[i].direction < 0 || ntts[i].direction > 3) return LZK_EINVAL;
+        groups[{ntts[i].log_n, ntts[i].direction}].push_back(reinterpret_cast<Fr*>(ntts[i].data));
+    }
+    LZK_TRY(ntt_prepare_launch());
+    for (auto& kv : groups) {
+        NttTables t; CosetTables c;
+        LZK_TRY(get_tables(kv.first.first, t, c));
+        for (size_t s0 = 0; s0 < kv.second.size(); s0 += 65535) {
+            size_t cnt = std::min<size_t>(65535, kv.second.size() - s0);
+            lzk_batch_plan::NGroup g{kv.first.first, kv.first.second, (uint32_t)cnt, nullptr};
+            if (cudaMalloc(&g.ptrs, sizeof(Fr*) * cnt) != cudaSuccess) { cudaGetLastError(); return LZK_ENOMEM; }
+            p->ngroups.push_back(g);
+            LZK_CUDA(cudaMemcpy(g.ptrs, kv.second.data() + s0, sizeof(Fr*) * cnt, cudaMemcpyHostToDevice));
+        }
+    }
+    LZK_CUDA(cudaStreamCreateWithFlags(&p->s_ntt, cudaStreamNonBlocking));
+    LZK_CUDA(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming));
+    LZK_CUDA(cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming));
+    return LZK_OK;
+}
+
+}  // namespace lzk
+
+using namespace lzk;
+
+extern "C" {
+
+int lzk_batch_plan_create(int group, const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_desc* ntts, size_t n_ntt,
+                          lzk_batch_plan** out)
+{
+    if (!out || (group != 1 && group != 2) || (n_msm && !msms) || (n_ntt && !ntts)) return LZK_EINVAL;
+    *out = nullptr;
+    lzk_batch_plan* p = new (std::nothrow) lzk_batch_plan();
+    if (!p) return LZK_ENOMEM;
+    p->group = group;
+    int rc = group == 2 ? create_plan<Fq2>(msms, n_msm, ntts, n_ntt, p) : create_plan<Fq>(msms, n_msm, ntts, n_ntt, p);
+    if (rc != LZK_OK) { destroy_plan(p); return rc; }
+    *out = p;
+    return LZK_OK;
+}
+
+int lzk_batch_plan_run(lzk_batch_plan* p, int use_graph, void* stream)
+{
+    if (!p) return LZK_EINVAL;
+    cudaStream_t st = as_stream(stream);
+    if (!use_graph) return run_all(p, st);
+    if (!st) return LZK_EINVAL;   // the legacy stream cannot be captured
+    if (!p->exec) {
+        LZK_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        int rc = run_all(p, st);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(st, &g);
+        if (rc != LZK_OK || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            return rc != LZK_OK ? rc : LZK_EDEVICE;
+        }
+        p->graph = g;
+        LZK_CUDA(cudaGraphInstantiate(&p->exec, g, 0));
+    }
+    LZK_CUDA(cudaGraphLaunch(p->exec, st));
+    return LZK_OK;
+}
+
+size_t lzk_batch_plan_device_bytes(const lzk_batch_plan* p) { return p ? p->ws_bytes : 0; }
+
+int lzk_batch_plan_destroy(lzk_batch_plan* p)
+{
+    if (!p) return LZK_EINVAL;
+    cudaDeviceSynchronize();
+    destroy_plan(p);
+    return LZK_OK;
+}
+
+}  // extern "C"

@@ -64,6 +64,9 @@ inline void plan_msm(MsmPlan& p, size_t n, uint32_t c, bool shared, size_t strid
 int msm_sort(const MsmPlan& p, const Fr* scalars, uint32_t* cnt, uint32_t* off, uint32_t* ent, uint32_t* bsums,
              cudaStream_t st);
 uint32_t msm_autotune(int group, size_t n, bool shared);
+// exclusive scan of cnt[0..B) into off[0..B], off[B] = total; bsums holds
+// (B + 4095) / 4096 + 1 words (msm_sort.cu)
+int scan_offsets(const uint32_t* cnt, uint32_t B, uint32_t* off, uint32_t* bsums, cudaStream_t st);
 
 // largest b in [lo, B) with off[b] <= e
 __device__ __forceinline__ uint32_t bucket_of(const uint32_t* off, uint32_t lo, uint32_t B, uint32_t e)

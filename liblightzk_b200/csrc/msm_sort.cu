@@ -153,6 +153,16 @@ __global__ void k_scan_add(uint32_t* __restrict__ off, uint32_t B, const uint32_
     for (uint64_t i = gtid(); i < B; i += gstride()) off[i] += bsums[i / kScanBlock];
 }
 
+int scan_offsets(const uint32_t* cnt, uint32_t B, uint32_t* off, uint32_t* bsums, cudaStream_t st)
+{
+    uint32_t nblk = (B + kScanBlock - 1) / kScanBlock;
+    if (nblk == 0) nblk = 1;
+    k_scan_local<<<nblk, 1024, 0, st>>>(cnt, B, off, bsums); note_launch();
+    k_scan_top<<<1, 1024, 0, st>>>(bsums, nblk, off, B); note_launch();
+    k_scan_add<<<grid_for(B, 256, 148 * 8), 256, 0, st>>>(off, B, bsums); note_launch();
+    return launch_status();
+}
+
 int msm_sort(const MsmPlan& p, const Fr* scalars, uint32_t* cnt, uint32_t* off, uint32_t* ent, uint32_t* bsums,
              cudaStream_t st)
 {
@@ -170,8 +180,16 @@ int msm_sort(const MsmPlan& p, const Fr* scalars, uint32_t* cnt, uint32_t* off, 
 // Cost model behind the default window width: mixed adds n*W(c) (8M+2S) plus
 // the reduction (two XYZZ adds per bucket, 12M+2S) plus, for plain bases,
 // the serial Horner doublings, weighted by their latency cost.
+// measured window widths by group and ceil(log2 n); 0 = use the model
+static uint8_t g_window_table[3][33];
+
 uint32_t msm_autotune(int group, size_t n, bool shared)
 {
+    if (!shared && n && group >= 1 && group <= 2) {
+        uint32_t lg = 0;
+        while (lg < 32 && (size_t(1) << lg) < n) lg++;
+        if (g_window_table[group][lg]) return g_window_table[group][lg];
+    }
     (void)group;
     if (n == 0) return 8;
     double best = 1e300; uint32_t bc = 8;
@@ -191,6 +209,13 @@ uint32_t msm_autotune(int group, size_t n, bool shared)
 using namespace lzk;
 
 extern "C" {
+
+int lzk_msm_set_window(int group, uint32_t log_n, uint32_t window_bits)
+{
+    if (group < 1 || group > 2 || log_n > 32 || (window_bits && (window_bits < 2 || window_bits > 24))) return LZK_EINVAL;
+    g_window_table[group][log_n] = (uint8_t)window_bits;
+    return LZK_OK;
+}
 
 uint32_t lzk_msm_precomp_windows(uint32_t window_bits) { return window_bits ? windows_for(window_bits) : 0; }
 

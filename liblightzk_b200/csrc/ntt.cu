@@ -149,11 +149,12 @@ __device__ __forceinline__ Fr coset_pow(const Fr* lo, const Fr* hi, size_t j)
 // per block.  `batch` transforms of size 2^k lie `bstride` elements apart.
 __global__ void __launch_bounds__(kNttThreads) k_ntt_pass(Fr* __restrict__ data, NttPass p, const Fr* __restrict__ tw,
                                                            uint32_t flags, const Fr* __restrict__ clo,
-                                                           const Fr* __restrict__ chi, size_t bstride)
+                                                           const Fr* __restrict__ chi, size_t bstride,
+                                                           Fr* const* __restrict__ ptrs)
 {
     extern __shared__ uint4 smem_raw[];
     Fr* sm = reinterpret_cast<Fr*>(smem_raw);
-    Fr* d = data + (size_t)blockIdx.y * bstride;
+    Fr* d = ptrs ? ptrs[blockIdx.y] : data + (size_t)blockIdx.y * bstride;
     const uint32_t G = 1u << p.m, R = p.R;
     const uint32_t rbits = __ffs(R) - 1;
     const size_t lowmask = (size_t(1) << p.lowbits) - 1;
@@ -198,9 +199,10 @@ __device__ __forceinline__ size_t brev_k(size_t j, uint32_t k)
 // In-place bit reversal; each output position pos is then multiplied by
 // scale (when non-null) and g^-pos (when clo != null).
 __global__ void k_ntt_bitrev(Fr* __restrict__ data, uint32_t k, const Fr* __restrict__ scale,
-                             const Fr* __restrict__ clo, const Fr* __restrict__ chi, size_t bstride)
+                             const Fr* __restrict__ clo, const Fr* __restrict__ chi, size_t bstride,
+                             Fr* const* __restrict__ ptrs)
 {
-    Fr* d = data + (size_t)blockIdx.y * bstride;
+    Fr* d = ptrs ? ptrs[blockIdx.y] : data + (size_t)blockIdx.y * bstride;
     size_t n = size_t(1) << k;
     Fr sc = scale ? ldg_elem(scale) : Fr::one();
     for (uint64_t j = gtid(); j < n; j += gstride()) {
@@ -215,21 +217,30 @@ __global__ void k_ntt_bitrev(Fr* __restrict__ data, uint32_t k, const Fr* __rest
     }
 }
 
-// Enqueue the passes of `count` transforms of size 2^k (natural order in,
-// natural order out) with twiddle table tw (w^e, e < n/2).
-static int ntt_enqueue(Fr* data, uint32_t k, uint32_t count, size_t bstride, const Fr* tw, const Fr* scale,
-                       const Fr* pre_lo, const Fr* pre_hi, const Fr* post_lo, const Fr* post_hi, cudaStream_t st)
+int ntt_prepare_launch()
 {
+    static std::mutex mu;
     static bool attr_set[64] = {false};
     int dev = 0;
     LZK_CUDA(cudaGetDevice(&dev));
-    if (dev < 64 && !attr_set[dev]) {
+    std::lock_guard<std::mutex> g(mu);
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
         LZK_CUDA(cudaFuncSetAttribute(k_ntt_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttElems * sizeof(Fr)));
         attr_set[dev] = true;
     }
+    return LZK_OK;
+}
+
+// Enqueue the passes of `count` transforms of size 2^k (natural order in,
+// natural order out) with twiddle table tw (w^e, e < n/2).
+static int ntt_enqueue(Fr* data, uint32_t k, uint32_t count, size_t bstride, const Fr* tw, const Fr* scale,
+                       const Fr* pre_lo, const Fr* pre_hi, const Fr* post_lo, const Fr* post_hi, cudaStream_t st,
+                       Fr* const* ptrs = nullptr)
+{
+    LZK_TRY(ntt_prepare_launch());
     if (k == 0) {
         if (scale || post_lo || pre_lo) {
-            k_ntt_bitrev<<<dim3(1, count), 32, 0, st>>>(data, 0, scale, post_lo, post_hi, bstride); note_launch();
+            k_ntt_bitrev<<<dim3(1, count), 32, 0, st>>>(data, 0, scale, post_lo, post_hi, bstride, ptrs); note_launch();
             return launch_status();
         }
         return LZK_OK;
@@ -250,24 +261,25 @@ static int ntt_enqueue(Fr* data, uint32_t k, uint32_t count, size_t bstride, con
         size_t blocks = (n >> m) / R;
         size_t smem = (size_t)G * R * sizeof(Fr);
         uint32_t flags = (q == 0 && pre_lo) ? NTT_PRE_COSET : 0u;
-        k_ntt_pass<<<dim3((unsigned)blocks, count), kNttThreads, smem, st>>>(data, pp, tw, flags, pre_lo, pre_hi, bstride); note_launch();
+        k_ntt_pass<<<dim3((unsigned)blocks, count), kNttThreads, smem, st>>>(data, pp, tw, flags, pre_lo, pre_hi, bstride, ptrs); note_launch();
         s0 += m;
     }
-    k_ntt_bitrev<<<dim3(grid_for(n, 256, 148 * 8), count), 256, 0, st>>>(data, k, scale, post_lo, post_hi, bstride); note_launch();
+    k_ntt_bitrev<<<dim3(grid_for(n, 256, 148 * 8), count), 256, 0, st>>>(data, k, scale, post_lo, post_hi, bstride, ptrs); note_launch();
     return launch_status();
 }
 
-int ntt_run(Fr* data, uint32_t k, int dir, uint32_t count, size_t bstride, const Fr* scale_override, cudaStream_t st)
+int ntt_run(Fr* data, uint32_t k, int dir, uint32_t count, size_t bstride, const Fr* scale_override, cudaStream_t st,
+            Fr* const* ptrs)
 {
-    if (!data || k > kNttMaxLog || dir < 0 || dir > 3 || count == 0 || count > 65535) return LZK_EINVAL;
-    if (count > 1 && bstride < (size_t(1) << k)) return LZK_EINVAL;
+    if ((!data && !ptrs) || k > kNttMaxLog || dir < 0 || dir > 3 || count == 0 || count > 65535) return LZK_EINVAL;
+    if (!ptrs && count > 1 && bstride < (size_t(1) << k)) return LZK_EINVAL;
     NttTables t; CosetTables c;
     LZK_TRY(get_tables(k, t, c));
     bool inv = dir & 1, coset = dir >= 2;
     const Fr* scale = scale_override ? scale_override : (inv ? t.consts + 2 : nullptr);
     return ntt_enqueue(data, k, count, bstride, t.tw[inv ? 1 : 0], scale,
                        (coset && !inv) ? c.lo[0] : nullptr, (coset && !inv) ? c.hi[0] : nullptr,
-                       (coset && inv) ? c.lo[1] : nullptr, (coset && inv) ? c.hi[1] : nullptr, st);
+                       (coset && inv) ? c.lo[1] : nullptr, (coset && inv) ? c.hi[1] : nullptr, st, ptrs);
 }
 
 }  // namespace lzk

@@ -17,9 +17,13 @@ struct CosetTables {
 
 // cached per-device tables for size 2^k (built synchronously on first use)
 int get_tables(uint32_t k, NttTables& out, CosetTables& cos);
-// count transforms of size 2^k, `bstride` apart; dir as LZK_NTT_*; a non-null
-// scale_override replaces the inverse's 2^-k factor (or adds a factor to a
-// forward transform)
-int ntt_run(Fr* data, uint32_t k, int dir, uint32_t count, size_t bstride, const Fr* scale_override, cudaStream_t st);
+// count transforms of size 2^k, `bstride` apart (or at ptrs[t], a device
+// table, when ptrs is non-null); dir as LZK_NTT_*; a non-null scale_override
+// replaces the inverse's 2^-k factor (or adds a factor to a forward transform)
+// one-time launch attributes (64 KB dynamic shared memory of the passes) on
+// the current device; done by the first transform, or ahead of stream capture
+int ntt_prepare_launch();
+int ntt_run(Fr* data, uint32_t k, int dir, uint32_t count, size_t bstride, const Fr* scale_override, cudaStream_t st,
+            Fr* const* ptrs = nullptr);
 
 }  // namespace lzk
