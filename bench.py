@@ -43,10 +43,12 @@ def parse():
     ap.add_argument("--mode", choices=["standard", "reference"], default="standard")
     ap.add_argument("--window", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", choices=["prove", "msm-g1", "msm-g2", "ntt", "batch"], default="prove",
+    ap.add_argument("--case", choices=["prove", "msm-g1", "msm-g2", "ntt", "batch", "serve"], default="prove",
                     help="prove = the benchmark; the others run one operator at --log-n for profiling")
     ap.add_argument("--log-n", type=int, default=20)
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--inflight", type=int, default=4)
+    ap.add_argument("--requests", type=int, default=48)
     return ap.parse_args()
 
 
@@ -225,6 +227,97 @@ def run_batch_case(args):
                       "tuned_windows": {lg: v[0] for lg, v in tuned.items()}}), flush=True)
 
 
+def run_serve_case(args):
+    """the serving workload: three resident circuits (2^16, 2^18, 2^20
+    constraints, built like the benchmark circuit), requests with witnesses
+    from pools of pre-solved witnesses (pinned host memory) and fresh (r, s);
+    capacity under a burst, latency under Poisson arrivals, and the plain
+    one-proof-at-a-time path on the same requests"""
+    import torch
+
+    from liblightzk_b200 import device, groth16, serve, synth
+    logs = [16, 18, 20]
+    provers, pools, circs = [], [], []
+    for lg in logs:
+        c = synth.Circuit(lg, seed=lg)
+        pk = synth.ProvingKey(c, seed=lg + 1)
+        provers.append(groth16.Prover(c, pk, mode=groth16.STANDARD, window_bits=args.window))
+        pools.append([torch.from_numpy(device.to_host(c.witness(1000 + i)).view(np.int64)).pin_memory()
+                      for i in range(4)])
+        circs.append(c)
+        del pk
+    torch.cuda.synchronize()
+    budget = 60 << 30
+    srv = serve.Server(budget, max_inflight=args.inflight)
+    cids = [srv.add(p) for p in provers]
+    rs = device.to_host(synth.random_fr(2 * args.requests, 9, 55)).reshape(args.requests, 2, 4)
+
+    def burst(which):
+        srv.reset_stats()
+        ids = [srv.submit(cids[w], pools[w][i % 4], rs[i, 0], rs[i, 1], pinned=True) for i, w in enumerate(which)]
+        srv.wait_idle()
+        for rid in ids:
+            srv.poll(rid)
+        return srv.stats()
+
+    def plain(which):
+        stream = torch.cuda.Stream()
+        zdev = [torch.empty((c.n_vars, 4), dtype=torch.int64, device="cuda") for c in circs]
+        proof = torch.empty(groth16.PROOF_WORDS, dtype=torch.int64, device="cuda")
+        torch.cuda.synchronize()
+        lat = []
+        t0 = time.perf_counter()
+        for i, w in enumerate(which):
+            t1 = time.perf_counter()
+            with torch.cuda.stream(stream):
+                zdev[w].copy_(pools[w][i % 4], non_blocking=True)
+            provers[w].prove(zdev[w], rs[i, 0], rs[i, 1], proof=proof, stream=stream)
+            stream.synchronize()
+            proof.cpu()
+            lat.append((time.perf_counter() - t1) * 1e3)
+        return len(which) / (time.perf_counter() - t0), lat
+
+    rng = np.random.default_rng(4)
+    mix = rng.integers(0, 3, args.requests)
+    for w in range(3):                     # warm-up: one context per slot and circuit
+        burst(np.full(args.inflight, w))
+    cap = burst(mix)
+    plain(mix[:6])
+    plain_pps, plain_lat = plain(mix)
+    only20 = np.full(min(args.requests, 24), 2)
+    cap20 = burst(only20)
+    plain20_pps, _ = plain(only20)
+    sweep = {}
+    for inflight in (1, 2, 3):
+        s2 = serve.Server(budget, max_inflight=inflight)
+        ids2 = [s2.add(p) for p in provers]
+        s2.reset_stats()
+        rids = [s2.submit(ids2[2], pools[2][i % 4], rs[i, 0], rs[i, 1], pinned=True) for i in range(12)]
+        s2.wait_idle()
+        for rid in rids:
+            s2.poll(rid)
+        sweep[inflight] = s2.stats()["proofs_per_s"]
+        s2.close()
+    poisson = []
+    for frac in (0.5, 0.85):
+        rate = frac * cap["proofs_per_s"]
+        st = serve.poisson_run(srv, cids, pools, rate, args.requests, seed=int(frac * 100))
+        poisson.append({"offered_per_s": rate, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+                        "proofs_per_s": st["proofs_per_s"], "completed": st["completed"]})
+    out = {"case": "serve", "circuits": [f"2^{lg}" for lg in logs], "max_inflight": args.inflight,
+           "requests": args.requests, "burst_mix": {"proofs_per_s": cap["proofs_per_s"], "p50_ms": cap["p50_ms"],
+                                                   "p99_ms": cap["p99_ms"]},
+           "plain_mix": {"proofs_per_s": plain_pps, "p50_ms": float(np.percentile(plain_lat, 50)),
+                         "p99_ms": float(np.percentile(plain_lat, 99))},
+           "served_over_plain_mix": cap["proofs_per_s"] / plain_pps,
+           "burst_2e20": {"proofs_per_s": cap20["proofs_per_s"], "p50_ms": cap20["p50_ms"], "p99_ms": cap20["p99_ms"]},
+           "plain_2e20_proofs_per_s": plain20_pps, "served_over_plain_2e20": cap20["proofs_per_s"] / plain20_pps,
+           "poisson": poisson, "device_bytes": srv.stats()["device_bytes"],
+           "inflight_sweep_2e20_proofs_per_s": sweep}
+    srv.close()
+    print(json.dumps(out), flush=True)
+
+
 def run_case(args):
     """one operator at 2^log_n, `reps` times, for profiling (prints ms)"""
     import torch
@@ -232,6 +325,8 @@ def run_case(args):
     from liblightzk_b200 import msm, ntt, synth
     if args.case == "batch":
         return run_batch_case(args)
+    if args.case == "serve":
+        return run_serve_case(args)
     n = 1 << args.log_n
     sc = synth.random_fr(n, 5, 77)
     out = []

@@ -38,7 +38,9 @@ extern "C" {
 #define LZK_ETIMEOUT     -3   /* a bounded device-side wait gave up */
 #define LZK_EDEVICE      -4   /* CUDA runtime error */
 #define LZK_EUNSUPPORTED -5   /* configuration not supported */
-#define LZK_EBUSY        -6   /* admission refused (memory budget) */
+#define LZK_EBUSY        -6   /* busy: pending, or refused by the memory budget */
+#define LZK_ECANCELED    -7   /* request cancelled before it started */
+#define LZK_EREJECTED    -8   /* request can never fit the memory budget */
 
 typedef struct { uint64_t limb[4]; } lzk_fr_t;
 typedef struct { uint64_t limb[4]; } lzk_fq_t;
@@ -267,6 +269,54 @@ size_t lzk_prover_device_bytes(const lzk_prover* prover);
  * proof: device memory. */
 int lzk_groth16_prove(lzk_prover* prover, const lzk_fr_t* z, const lzk_fr_t* r, const lzk_fr_t* s,
                       lzk_groth16_proof* proof, void* stream);
+
+/* -------------------------------------------------------------- serving
+ * A prove-request server over resident provers with continuous batching.
+ * A worker thread admits queued requests (oldest first) into proof
+ * contexts -- an idle context of the request's circuit, or a new one while
+ * the device-memory budget allows (idle contexts of other circuits are
+ * released to make room) -- and runs each on its own streams, so requests
+ * that arrive while others run start as soon as a context and memory are
+ * free and their work overlaps on the device.  Resident provers count
+ * against the budget when added.  Latency is submission to completion.
+ * New relative to the reference, which proves once per process
+ * (groth16.cuh:48-222). */
+typedef struct lzk_server lzk_server;
+
+typedef struct lzk_server_cfg {
+    size_t hbm_budget_bytes;   /* resident provers + all proof contexts */
+    uint32_t max_inflight;     /* proofs running at once */
+    uint32_t reserved;
+} lzk_server_cfg;
+
+typedef struct lzk_server_stats {
+    uint64_t submitted, completed, rejected, cancelled, queued, running;
+    size_t device_bytes;       /* resident + contexts in use or cached */
+    double p50_ms, p99_ms, mean_ms, max_ms;
+    double proofs_per_s;       /* completed / (last completion - first submission) */
+} lzk_server_stats;
+
+/* the witness is pinned host memory that stays unchanged until the request
+ * completes (otherwise the server copies it at submission) */
+#define LZK_REQ_WITNESS_PINNED 0x1u
+
+int lzk_server_create(const lzk_server_cfg* cfg, lzk_server** out);
+/* The prover stays owned by the caller and must outlive the server. */
+int lzk_server_add_circuit(lzk_server* server, lzk_prover* prover, uint32_t* circuit_id);
+/* z: HOST witness (n_vars Fr); r, s: host values. */
+int lzk_server_submit(lzk_server* server, uint32_t circuit_id, const lzk_fr_t* z, const lzk_fr_t* r,
+                      const lzk_fr_t* s, uint32_t flags, uint64_t* request_id);
+/* LZK_OK: done, *proof (host) filled, request forgotten; LZK_EBUSY: not done;
+ * LZK_ECANCELED / LZK_EREJECTED: finished without a proof (forgotten). */
+int lzk_server_poll(lzk_server* server, uint64_t request_id, lzk_groth16_proof* proof, double* latency_ms);
+/* cancel a request that has not started (LZK_EBUSY once it has) */
+int lzk_server_cancel(lzk_server* server, uint64_t request_id);
+/* wait until nothing is queued or running; LZK_ETIMEOUT after timeout_ms */
+int lzk_server_wait_idle(lzk_server* server, int timeout_ms);
+int lzk_server_get_stats(lzk_server* server, lzk_server_stats* stats);
+int lzk_server_reset_stats(lzk_server* server);
+/* drops queued requests, waits for running ones, frees all contexts */
+int lzk_server_destroy(lzk_server* server);
 
 /* ------------------------------------------------------------ batching
  * Many MSMs (one group: 1 = G1, 2 = G2; plain affine bases) and NTTs of

@@ -44,6 +44,15 @@ SIGNATURES = {
     "lzk_prover_destroy": (c_i, [c_p]),
     "lzk_prover_device_bytes": (c_sz, [c_p]),
     "lzk_groth16_prove": (c_i, [c_p, c_p, c_p, c_p, c_p, c_p]),
+    "lzk_server_create": (c_i, [c_p, c_p]),
+    "lzk_server_add_circuit": (c_i, [c_p, c_p, c_p]),
+    "lzk_server_submit": (c_i, [c_p, c_u32, c_p, c_p, c_p, c_u32, c_p]),
+    "lzk_server_poll": (c_i, [c_p, ctypes.c_uint64, c_p, c_p]),
+    "lzk_server_cancel": (c_i, [c_p, ctypes.c_uint64]),
+    "lzk_server_wait_idle": (c_i, [c_p, c_i]),
+    "lzk_server_get_stats": (c_i, [c_p, c_p]),
+    "lzk_server_reset_stats": (c_i, [c_p]),
+    "lzk_server_destroy": (c_i, [c_p]),
     "lzk_batch_plan_create": (c_i, [c_i, c_p, c_sz, c_p, c_sz, c_p]),
     "lzk_batch_plan_run": (c_i, [c_p, c_i, c_p]),
     "lzk_batch_plan_device_bytes": (c_sz, [c_p]),

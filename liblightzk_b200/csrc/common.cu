@@ -34,7 +34,9 @@ const char* lzk_status_string(int status)
         case LZK_ETIMEOUT: return "bounded device wait timed out";
         case LZK_EDEVICE: return "CUDA runtime error";
         case LZK_EUNSUPPORTED: return "unsupported configuration";
-        case LZK_EBUSY: return "admission refused by the memory budget";
+        case LZK_EBUSY: return "busy (pending, or refused by the memory budget)";
+        case LZK_ECANCELED: return "request cancelled";
+        case LZK_EREJECTED: return "request can never fit the memory budget";
         default: return "unknown status";
     }
 }

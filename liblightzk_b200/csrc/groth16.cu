@@ -32,40 +32,8 @@
 #include "msm.cuh"
 #include "ntt.cuh"
 #include "keygen.cuh"
-#include "r1cs.cuh"
+#include "prover.cuh"
 #include <new>
-
-struct lzk_prover {
-    int mode = 0;
-    lzk::CsrDev A, B, C;
-    uint64_t rows = 0, n_vars = 0, n_public = 0;
-    uint32_t log_m = 0;
-    size_t M = 0;
-    // shifted-copy tables: a, b1, l, h (G1) and b2 (G2)
-    lzk::Aff<lzk::Fq>* tab[4] = {nullptr, nullptr, nullptr, nullptr};
-    size_t tn[4] = {0, 0, 0, 0};
-    lzk::Aff<lzk::Fq2>* tab2 = nullptr;
-    size_t tn2 = 0;
-    uint32_t c = 16, wins = 16;
-    // constants in device memory
-    lzk::Aff<lzk::Fq>* g1c = nullptr;   // alpha1, beta1, delta1
-    lzk::Aff<lzk::Fq2>* g2c = nullptr;  // beta2, delta2
-    lzk::Fr* zinv = nullptr;            // (g^M - 1)^-1
-    // scratch
-    lzk::Fr* x = nullptr;               // 3 * L
-    size_t L = 0;
-    lzk::Jac<lzk::Fq>* g1res = nullptr;   // A, B1, L, H MSM results
-    lzk::Jac<lzk::Fq2>* g2res = nullptr;  // B2 MSM result
-    lzk::XYZZ<lzk::Fq>* sm1 = nullptr;    // r d1, s a1, r b1, (r s) d1, s A, r B1
-    lzk::XYZZ<lzk::Fq2>* sm2 = nullptr;   // s d2
-    lzk::Aff<lzk::Fq>* comb1 = nullptr;   // comb tables of a1, b1, d1 (3 x 8192)
-    lzk::Aff<lzk::Fq2>* comb2 = nullptr;  // comb table of d2
-    void* ws[3] = {nullptr, nullptr, nullptr};
-    size_t wsb[3] = {0, 0, 0};
-    cudaStream_t s1 = nullptr, s2 = nullptr, s3 = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_b1 = nullptr, ev_s1 = nullptr, ev_s2 = nullptr, ev_s3 = nullptr;
-    size_t bytes = 0;
-};
 
 namespace lzk {
 
@@ -176,29 +144,81 @@ static Scal to_scal(const lzk_fr_t* f)
     return s;
 }
 
-static void destroy(lzk_prover* p)
-{
-    if (!p) return;
-    for (auto t : p->tab) if (t) cudaFree(t);
-    if (p->tab2) cudaFree(p->tab2);
-    for (auto w : p->ws) if (w) cudaFree(w);
-    void* misc[] = {p->g1c, p->g2c, p->zinv, p->x, p->g1res, p->g2res, p->sm1, p->sm2, p->comb1, p->comb2};
-    for (auto m : misc) if (m) cudaFree(m);
-    if (p->s1) cudaStreamDestroy(p->s1);
-    if (p->s2) cudaStreamDestroy(p->s2);
-    if (p->s3) cudaStreamDestroy(p->s3);
-    cudaEvent_t evs[] = {p->ev_fork, p->ev_b1, p->ev_s1, p->ev_s2, p->ev_s3};
-    for (auto e : evs) if (e) cudaEventDestroy(e);
-    delete p;
-}
-
 template <class T>
-static int dalloc(lzk_prover* p, T** ptr, size_t count)
+static int dalloc(size_t* acct, T** ptr, size_t count)
 {
     size_t b = count * sizeof(T);
     if (cudaMalloc(reinterpret_cast<void**>(ptr), b ? b : 16) != cudaSuccess) { cudaGetLastError(); return LZK_ENOMEM; }
-    p->bytes += b;
+    *acct += b;
     return LZK_OK;
+}
+
+void ctx_destroy(ProveCtx* x)
+{
+    if (!x) return;
+    for (auto w : x->ws) if (w) cudaFree(w);
+    void* misc[] = {x->x, x->g1res, x->g2res, x->sm1, x->sm2, x->z, x->proof};
+    for (auto m : misc) if (m) cudaFree(m);
+    if (x->proof_host) cudaFreeHost(x->proof_host);
+    if (x->ev_done) cudaEventDestroy(x->ev_done);
+    cudaStream_t sts[] = {x->s0, x->s1, x->s2, x->s3};
+    for (auto t : sts) if (t) cudaStreamDestroy(t);
+    cudaEvent_t evs[] = {x->ev_fork, x->ev_b1, x->ev_s1, x->ev_s2, x->ev_s3};
+    for (auto e : evs) if (e) cudaEventDestroy(e);
+    delete x;
+}
+
+// Scratch for one proof of prover p; serving contexts also get their own
+// main stream and witness and proof buffers.
+int ctx_create(const lzk_prover* p, bool serving, ProveCtx** out)
+{
+    *out = nullptr;
+    ProveCtx* x = new (std::nothrow) ProveCtx();
+    if (!x) return LZK_ENOMEM;
+    int rc = LZK_OK;
+    do {
+        if ((rc = dalloc(&x->bytes, &x->x, 3 * p->L))) break;
+        if ((rc = dalloc(&x->bytes, &x->g1res, 4))) break;
+        if ((rc = dalloc(&x->bytes, &x->g2res, 1))) break;
+        if ((rc = dalloc(&x->bytes, &x->sm1, 6))) break;
+        if ((rc = dalloc(&x->bytes, &x->sm2, 1))) break;
+        for (int i = 0; i < 3 && rc == LZK_OK; i++) {
+            lzk_msm_cfg cfg{};
+            cfg.window_bits = p->c;
+            cfg.flags = LZK_MSM_PRECOMPUTED;
+            cfg.precomp_windows = p->wins;
+            size_t mx = p->M > p->n_vars ? p->M : p->n_vars;
+            cfg.level_stride = mx;
+            x->wsb[i] = lzk_msm_workspace_bytes(i == 2 ? 2 : 1, mx, &cfg);
+            rc = dalloc(&x->bytes, reinterpret_cast<char**>(&x->ws[i]), x->wsb[i]);
+        }
+        if (rc) break;
+        if (serving) {
+            if ((rc = dalloc(&x->bytes, &x->z, p->n_vars))) break;
+            if ((rc = dalloc(&x->bytes, &x->proof, 1))) break;
+            if (cudaStreamCreateWithFlags(&x->s0, cudaStreamNonBlocking) != cudaSuccess) { rc = LZK_EDEVICE; break; }
+            if (cudaEventCreateWithFlags(&x->ev_done, cudaEventDisableTiming) != cudaSuccess) { rc = LZK_EDEVICE; break; }
+            if (cudaMallocHost(&x->proof_host, sizeof(lzk_groth16_proof)) != cudaSuccess) { rc = LZK_ENOMEM; break; }
+        }
+        cudaStream_t* sts[] = {&x->s1, &x->s2, &x->s3};
+        for (auto t : sts) if (cudaStreamCreateWithFlags(t, cudaStreamNonBlocking) != cudaSuccess) rc = LZK_EDEVICE;
+        cudaEvent_t* evs[] = {&x->ev_fork, &x->ev_b1, &x->ev_s1, &x->ev_s2, &x->ev_s3};
+        for (auto e : evs) if (cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess) rc = LZK_EDEVICE;
+    } while (0);
+    if (rc != LZK_OK) { cudaGetLastError(); ctx_destroy(x); return rc; }
+    *out = x;
+    return LZK_OK;
+}
+
+static void destroy(lzk_prover* p)
+{
+    if (!p) return;
+    ctx_destroy(p->ctx0);
+    for (auto t : p->tab) if (t) cudaFree(t);
+    if (p->tab2) cudaFree(p->tab2);
+    void* misc[] = {p->g1c, p->g2c, p->zinv, p->comb1, p->comb2};
+    for (auto m : misc) if (m) cudaFree(m);
+    delete p;
 }
 
 static int create(const lzk_groth16_circuit* c, const lzk_groth16_pk* pk, int mode, uint32_t window_bits, lzk_prover* p)
@@ -211,6 +231,7 @@ static int create(const lzk_groth16_circuit* c, const lzk_groth16_pk* pk, int mo
     p->mode = mode;
     p->log_m = c->log_domain;
     p->M = size_t(1) << c->log_domain;
+    p->L = mode == LZK_PROVE_REFERENCE ? 2 * p->M : p->M;
     p->rows = c->A.rows;
     if (c->A.rows > p->M || c->B.rows > p->M || c->C.rows > p->M) return LZK_EINVAL;
     p->n_vars = c->n_vars;
@@ -221,57 +242,35 @@ static int create(const lzk_groth16_circuit* c, const lzk_groth16_pk* pk, int mo
     if (p->c < 2 || p->c > 24) return LZK_EINVAL;
     p->wins = windows_for(p->c);
 
-    LZK_CUDA(cudaStreamCreateWithFlags(&p->s1, cudaStreamNonBlocking));
-    LZK_CUDA(cudaStreamCreateWithFlags(&p->s2, cudaStreamNonBlocking));
-    LZK_CUDA(cudaStreamCreateWithFlags(&p->s3, cudaStreamNonBlocking));
-    cudaEvent_t* evs[] = {&p->ev_fork, &p->ev_b1, &p->ev_s1, &p->ev_s2, &p->ev_s3};
-    for (auto e : evs) LZK_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
-    cudaStream_t st = p->s1;
+    LZK_TRY(ctx_create(p, false, &p->ctx0));
+    cudaStream_t st = p->ctx0->s1;
 
     // tables
     const lzk_g1_affine_t* q1[4] = {pk->a_query, pk->b1_query, pk->l_query, pk->h_query};
     size_t n1[4] = {c->n_vars, c->n_vars, c->n_vars - c->n_public - 1, p->M - 1};
     for (int q = 0; q < 4; q++) {
         p->tn[q] = n1[q];
-        LZK_TRY(dalloc(p, &p->tab[q], (size_t)p->wins * (n1[q] ? n1[q] : 1)));
+        LZK_TRY(dalloc(&p->bytes, &p->tab[q], (size_t)p->wins * (n1[q] ? n1[q] : 1)));
         if (n1[q])
             LZK_TRY(lzk_g1_precompute(q1[q], n1[q], p->c, p->wins, reinterpret_cast<lzk_g1_affine_t*>(p->tab[q]), n1[q], st));
     }
     p->tn2 = c->n_vars;
-    LZK_TRY(dalloc(p, &p->tab2, (size_t)p->wins * p->tn2));
+    LZK_TRY(dalloc(&p->bytes, &p->tab2, (size_t)p->wins * p->tn2));
     LZK_TRY(lzk_g2_precompute(pk->b2_query, p->tn2, p->c, p->wins, reinterpret_cast<lzk_g2_affine_t*>(p->tab2), p->tn2, st));
 
     // constants
-    LZK_TRY(dalloc(p, &p->g1c, 3));
-    LZK_TRY(dalloc(p, &p->g2c, 2));
+    LZK_TRY(dalloc(&p->bytes, &p->g1c, 3));
+    LZK_TRY(dalloc(&p->bytes, &p->g2c, 2));
     const lzk_g1_affine_t g1h[3] = {pk->alpha1, pk->beta1, pk->delta1};
     const lzk_g2_affine_t g2h[2] = {pk->beta2, pk->delta2};
     LZK_CUDA(cudaMemcpyAsync(p->g1c, g1h, sizeof(g1h), cudaMemcpyHostToDevice, st));
     LZK_CUDA(cudaMemcpyAsync(p->g2c, g2h, sizeof(g2h), cudaMemcpyHostToDevice, st));
-    LZK_TRY(dalloc(p, &p->zinv, 1));
+    LZK_TRY(dalloc(&p->bytes, &p->zinv, 1));
     k_zinv<<<1, 32, 0, st>>>(p->log_m, p->zinv); note_launch();
-
-    // scratch
-    p->L = mode == LZK_PROVE_REFERENCE ? 2 * p->M : p->M;
-    LZK_TRY(dalloc(p, &p->x, 3 * p->L));
-    LZK_TRY(dalloc(p, &p->g1res, 4));
-    LZK_TRY(dalloc(p, &p->g2res, 1));
-    LZK_TRY(dalloc(p, &p->sm1, 6));
-    LZK_TRY(dalloc(p, &p->comb1, 3 * 8192));
-    LZK_TRY(dalloc(p, &p->comb2, 8192));
+    LZK_TRY(dalloc(&p->bytes, &p->comb1, 3 * 8192));
+    LZK_TRY(dalloc(&p->bytes, &p->comb2, 8192));
     for (int i = 0; i < 3; i++) LZK_TRY(comb_build<Fq>(p->g1c + i, p->comb1 + i * 8192, st));
     LZK_TRY(comb_build<Fq2>(p->g2c + 1, p->comb2, st));
-    LZK_TRY(dalloc(p, &p->sm2, 1));
-    for (int i = 0; i < 3; i++) {
-        lzk_msm_cfg cfg{};
-        cfg.window_bits = p->c;
-        cfg.flags = LZK_MSM_PRECOMPUTED;
-        cfg.precomp_windows = p->wins;
-        cfg.level_stride = p->M + c->n_vars;
-        size_t mx = p->M > c->n_vars ? p->M : c->n_vars;
-        p->wsb[i] = lzk_msm_workspace_bytes(i == 2 ? 2 : 1, mx, &cfg);
-        LZK_TRY(dalloc(p, reinterpret_cast<char**>(&p->ws[i]), p->wsb[i]));
-    }
     // NTT tables for every size the chain uses
     NttTables t; CosetTables ct;
     LZK_TRY(get_tables(p->log_m, t, ct));
@@ -284,32 +283,33 @@ static int create(const lzk_groth16_circuit* c, const lzk_groth16_pk* pk, int mo
     return LZK_OK;
 }
 
-static int msm_tab1(lzk_prover* p, int q, const Fr* scal, size_t n, Jac<Fq>* out, int wsi, cudaStream_t st)
+static int msm_tab1(const lzk_prover* p, ProveCtx* x, int q, const Fr* scal, size_t n, Jac<Fq>* out, int wsi,
+                    cudaStream_t st)
 {
     lzk_msm_cfg cfg{};
     cfg.window_bits = p->c;
     cfg.flags = LZK_MSM_PRECOMPUTED;
     cfg.precomp_windows = p->wins;
     cfg.level_stride = p->tn[q];
-    cfg.workspace = p->ws[wsi];
-    cfg.workspace_bytes = p->wsb[wsi];
+    cfg.workspace = x->ws[wsi];
+    cfg.workspace_bytes = x->wsb[wsi];
     return lzk_msm_g1(reinterpret_cast<const lzk_fr_t*>(scal), reinterpret_cast<const lzk_g1_affine_t*>(p->tab[q]), n,
                       reinterpret_cast<lzk_g1_t*>(out), &cfg, st);
 }
 
-static int prove(lzk_prover* p, const Fr* z, const lzk_fr_t* r, const lzk_fr_t* s, lzk_groth16_proof* proof,
-                 cudaStream_t st)
+int prove_ctx(const lzk_prover* p, ProveCtx* x, const Fr* z, const lzk_fr_t* r, const lzk_fr_t* s,
+              lzk_groth16_proof* proof, cudaStream_t st)
 {
     if (!p || !z || !r || !s || !proof) return LZK_EINVAL;
     Scal rs = to_scal(r), ss = to_scal(s);
     void* tr = trace_begin("groth16_prove", st);
-    LZK_CUDA(cudaEventRecord(p->ev_fork, st));
-    LZK_CUDA(cudaStreamWaitEvent(p->s1, p->ev_fork, 0));
-    LZK_CUDA(cudaStreamWaitEvent(p->s2, p->ev_fork, 0));
-    LZK_CUDA(cudaStreamWaitEvent(p->s3, p->ev_fork, 0));
+    LZK_CUDA(cudaEventRecord(x->ev_fork, st));
+    LZK_CUDA(cudaStreamWaitEvent(x->s1, x->ev_fork, 0));
+    LZK_CUDA(cudaStreamWaitEvent(x->s2, x->ev_fork, 0));
+    LZK_CUDA(cudaStreamWaitEvent(x->s3, x->ev_fork, 0));
 
     // s3: fixed-base products
-    k_fixed_products<<<1, 32, 0, p->s3>>>(p->comb1, p->comb2, rs, ss, p->sm1, p->sm2); note_launch();
+    k_fixed_products<<<1, 32, 0, x->s3>>>(p->comb1, p->comb2, rs, ss, x->sm1, x->sm2); note_launch();
 
     // s2: the G2 MSM
     {
@@ -318,29 +318,29 @@ static int prove(lzk_prover* p, const Fr* z, const lzk_fr_t* r, const lzk_fr_t* 
         cfg.flags = LZK_MSM_PRECOMPUTED;
         cfg.precomp_windows = p->wins;
         cfg.level_stride = p->tn2;
-        cfg.workspace = p->ws[2];
-        cfg.workspace_bytes = p->wsb[2];
+        cfg.workspace = x->ws[2];
+        cfg.workspace_bytes = x->wsb[2];
         LZK_TRY(lzk_msm_g2(reinterpret_cast<const lzk_fr_t*>(z), reinterpret_cast<const lzk_g2_affine_t*>(p->tab2),
-                           p->n_vars, reinterpret_cast<lzk_g2_t*>(p->g2res), &cfg, p->s2));
+                           p->n_vars, reinterpret_cast<lzk_g2_t*>(x->g2res), &cfg, x->s2));
     }
-    LZK_CUDA(cudaEventRecord(p->ev_s2, p->s2));
+    LZK_CUDA(cudaEventRecord(x->ev_s2, x->s2));
 
     // s1: A, B1 and L MSMs; s3 picks up A and B1 for s*A and r*B1
-    LZK_TRY(msm_tab1(p, 0, z, p->n_vars, p->g1res + 0, 1, p->s1));
-    LZK_TRY(msm_tab1(p, 1, z, p->n_vars, p->g1res + 1, 1, p->s1));
-    LZK_CUDA(cudaEventRecord(p->ev_b1, p->s1));
-    LZK_CUDA(cudaStreamWaitEvent(p->s3, p->ev_b1, 0));
-    k_dep_products<<<1, 32, 0, p->s3>>>(p->g1res, rs, ss, p->sm1); note_launch();
-    LZK_CUDA(cudaEventRecord(p->ev_s3, p->s3));
+    LZK_TRY(msm_tab1(p, x, 0, z, p->n_vars, x->g1res + 0, 1, x->s1));
+    LZK_TRY(msm_tab1(p, x, 1, z, p->n_vars, x->g1res + 1, 1, x->s1));
+    LZK_CUDA(cudaEventRecord(x->ev_b1, x->s1));
+    LZK_CUDA(cudaStreamWaitEvent(x->s3, x->ev_b1, 0));
+    k_dep_products<<<1, 32, 0, x->s3>>>(x->g1res, rs, ss, x->sm1); note_launch();
+    LZK_CUDA(cudaEventRecord(x->ev_s3, x->s3));
     size_t nl = p->n_vars - p->n_public - 1;
-    LZK_TRY(msm_tab1(p, 2, z + p->n_public + 1, nl, p->g1res + 2, 1, p->s1));
-    LZK_CUDA(cudaEventRecord(p->ev_s1, p->s1));
+    LZK_TRY(msm_tab1(p, x, 2, z + p->n_public + 1, nl, x->g1res + 2, 1, x->s1));
+    LZK_CUDA(cudaEventRecord(x->ev_s1, x->s1));
 
     // main: H polynomial and H MSM
-    Fr* x0 = p->x;
-    Fr* x1 = p->x + p->L;
-    Fr* x2 = p->x + 2 * p->L;
-    LZK_CUDA(cudaMemsetAsync(p->x, 0, 3 * p->L * sizeof(Fr), st));
+    Fr* x0 = x->x;
+    Fr* x1 = x->x + p->L;
+    Fr* x2 = x->x + 2 * p->L;
+    LZK_CUDA(cudaMemsetAsync(x->x, 0, 3 * p->L * sizeof(Fr), st));
     lzk_csr none{};
     (void)none;
     {
@@ -353,27 +353,27 @@ static int prove(lzk_prover* p, const Fr* z, const lzk_fr_t* r, const lzk_fr_t* 
     }
     const Fr* hs;
     if (p->mode == LZK_PROVE_REFERENCE) {
-        LZK_TRY(ntt_run(p->x, p->log_m, LZK_NTT_INVERSE, 3, p->L, nullptr, st));
-        LZK_TRY(ntt_run(p->x, p->log_m + 1, LZK_NTT_FORWARD, 3, p->L, nullptr, st));
+        LZK_TRY(ntt_run(x->x, p->log_m, LZK_NTT_INVERSE, 3, p->L, nullptr, st));
+        LZK_TRY(ntt_run(x->x, p->log_m + 1, LZK_NTT_FORWARD, 3, p->L, nullptr, st));
         k_abc<<<grid_for(p->L, 256, 148 * 8), 256, 0, st>>>(x0, x1, x2, p->L, nullptr); note_launch();
         NttTables t4; CosetTables ct;
         LZK_TRY(get_tables(p->log_m + 2, t4, ct));
         LZK_TRY(ntt_run(x0, p->log_m + 1, LZK_NTT_INVERSE, 1, 0, t4.consts + 2, st));
         hs = x0 + p->M + 1;
     } else {
-        LZK_TRY(ntt_run(p->x, p->log_m, LZK_NTT_INVERSE, 3, p->L, nullptr, st));
-        LZK_TRY(ntt_run(p->x, p->log_m, LZK_NTT_COSET_FORWARD, 3, p->L, nullptr, st));
+        LZK_TRY(ntt_run(x->x, p->log_m, LZK_NTT_INVERSE, 3, p->L, nullptr, st));
+        LZK_TRY(ntt_run(x->x, p->log_m, LZK_NTT_COSET_FORWARD, 3, p->L, nullptr, st));
         k_abc<<<grid_for(p->L, 256, 148 * 8), 256, 0, st>>>(x0, x1, x2, p->L, p->zinv); note_launch();
         LZK_TRY(ntt_run(x0, p->log_m, LZK_NTT_COSET_INVERSE, 1, 0, nullptr, st));
         hs = x0;
     }
-    LZK_TRY(msm_tab1(p, 3, hs, p->M - 1, p->g1res + 3, 0, st));
+    LZK_TRY(msm_tab1(p, x, 3, hs, p->M - 1, x->g1res + 3, 0, st));
 
     // join and assemble
-    LZK_CUDA(cudaStreamWaitEvent(st, p->ev_s1, 0));
-    LZK_CUDA(cudaStreamWaitEvent(st, p->ev_s2, 0));
-    LZK_CUDA(cudaStreamWaitEvent(st, p->ev_s3, 0));
-    k_assemble<<<1, 32, 0, st>>>(p->g1c, p->g2c, p->g1res, p->g2res, p->sm1, p->sm2, proof); note_launch();
+    LZK_CUDA(cudaStreamWaitEvent(st, x->ev_s1, 0));
+    LZK_CUDA(cudaStreamWaitEvent(st, x->ev_s2, 0));
+    LZK_CUDA(cudaStreamWaitEvent(st, x->ev_s3, 0));
+    k_assemble<<<1, 32, 0, st>>>(p->g1c, p->g2c, x->g1res, x->g2res, x->sm1, x->sm2, proof); note_launch();
     trace_end(tr, st);
     return launch_status();
 }
@@ -405,7 +405,7 @@ int lzk_prover_destroy(lzk_prover* p)
     return LZK_OK;
 }
 
-size_t lzk_prover_device_bytes(const lzk_prover* p) { return p ? p->bytes : 0; }
+size_t lzk_prover_device_bytes(const lzk_prover* p) { return p ? p->bytes + (p->ctx0 ? p->ctx0->bytes : 0) : 0; }
 
 int lzk_poly_a_times_b_minus_c(lzk_fr_t* A, const lzk_fr_t* B, const lzk_fr_t* C, size_t n, void* stream)
 {
@@ -419,7 +419,8 @@ int lzk_poly_a_times_b_minus_c(lzk_fr_t* A, const lzk_fr_t* B, const lzk_fr_t* C
 int lzk_groth16_prove(lzk_prover* p, const lzk_fr_t* z, const lzk_fr_t* r, const lzk_fr_t* s,
                       lzk_groth16_proof* proof, void* stream)
 {
-    return prove(p, reinterpret_cast<const Fr*>(z), r, s, proof, as_stream(stream));
+    if (!p) return LZK_EINVAL;
+    return prove_ctx(p, p->ctx0, reinterpret_cast<const Fr*>(z), r, s, proof, as_stream(stream));
 }
 
 }  // extern "C"

@@ -1,0 +1,63 @@
+// prover.cuh -- the Groth16 prover's resident state and per-proof contexts,
+// shared by the prove chain (groth16.cu) and the serving loop (server.cu).
+#pragma once
+#include "common.cuh"
+#include "curve.cuh"
+#include "r1cs.cuh"
+
+namespace lzk {
+
+// Scratch and streams of one proof in flight.  A prover owns one (used by
+// lzk_groth16_prove); the serving loop creates more, one per admitted
+// request, all sharing the prover's resident tables.
+struct ProveCtx {
+    Fr* x = nullptr;                  // 3 * L: A z, B z, C z and the H polynomial
+    Jac<Fq>* g1res = nullptr;         // A, B1, L, H MSM results
+    Jac<Fq2>* g2res = nullptr;        // B2 MSM result
+    XYZZ<Fq>* sm1 = nullptr;          // r d1, s a1, r b1, (r s) d1, s A, r B1
+    XYZZ<Fq2>* sm2 = nullptr;         // s d2
+    void* ws[3] = {nullptr, nullptr, nullptr};
+    size_t wsb[3] = {0, 0, 0};
+    Fr* z = nullptr;                  // witness buffer (serving contexts only)
+    lzk_groth16_proof* proof = nullptr;   // proof buffer (serving contexts only)
+    lzk_groth16_proof* proof_host = nullptr;   // pinned copy target (serving contexts only)
+    cudaEvent_t ev_done = nullptr;             // end of the proof on s0 (serving contexts only)
+    cudaStream_t s0 = nullptr, s1 = nullptr, s2 = nullptr, s3 = nullptr;   // s0: serving contexts only
+    cudaEvent_t ev_fork = nullptr, ev_b1 = nullptr, ev_s1 = nullptr, ev_s2 = nullptr, ev_s3 = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace lzk
+
+struct lzk_prover {
+    int mode = 0;
+    lzk::CsrDev A, B, C;
+    uint64_t rows = 0, n_vars = 0, n_public = 0;
+    uint32_t log_m = 0;
+    size_t M = 0, L = 0;
+    // shifted-copy tables: a, b1, l, h (G1) and b2 (G2)
+    lzk::Aff<lzk::Fq>* tab[4] = {nullptr, nullptr, nullptr, nullptr};
+    size_t tn[4] = {0, 0, 0, 0};
+    lzk::Aff<lzk::Fq2>* tab2 = nullptr;
+    size_t tn2 = 0;
+    uint32_t c = 16, wins = 16;
+    // constants in device memory
+    lzk::Aff<lzk::Fq>* g1c = nullptr;   // alpha1, beta1, delta1
+    lzk::Aff<lzk::Fq2>* g2c = nullptr;  // beta2, delta2
+    lzk::Fr* zinv = nullptr;            // (g^M - 1)^-1
+    lzk::Aff<lzk::Fq>* comb1 = nullptr;   // comb tables of a1, b1, d1 (3 x 8192)
+    lzk::Aff<lzk::Fq2>* comb2 = nullptr;  // comb table of d2
+    lzk::ProveCtx* ctx0 = nullptr;
+    size_t bytes = 0;       // resident bytes (tables, constants)
+};
+
+namespace lzk {
+
+// scratch (and, for serving, streams and witness/proof buffers) of one proof
+int ctx_create(const lzk_prover* p, bool serving, ProveCtx** out);
+void ctx_destroy(ProveCtx* x);
+// enqueue one proof on stream st using context x (x's side streams join st)
+int prove_ctx(const lzk_prover* p, ProveCtx* x, const Fr* z, const lzk_fr_t* r, const lzk_fr_t* s,
+              lzk_groth16_proof* proof, cudaStream_t st);
+
+}  // namespace lzk
