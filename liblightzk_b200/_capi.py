@@ -7,7 +7,8 @@ import ctypes
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "liblzk_b200.so")
+# LZK_LIBRARY selects another build of the library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("LZK_LIBRARY") or os.path.join(_HERE, "liblzk_b200.so")
 
 c_p = ctypes.c_void_p
 c_sz = ctypes.c_size_t

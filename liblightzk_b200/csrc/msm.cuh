@@ -9,7 +9,7 @@ namespace lzk {
 struct G1 { using F = Fq; };
 struct G2 { using F = Fq2; };
 
-constexpr uint32_t kAccChunk = 32;   // sorted entries per accumulation thread
+constexpr uint32_t kAccChunk = 64;   // sorted entries per accumulation thread
 constexpr uint32_t kLevelL = 32;     // buckets per warp in a reduction level
 constexpr uint32_t kFixSmall = 64;   // partials a single fix-up thread folds
 
