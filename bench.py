@@ -15,6 +15,7 @@ libff-derived host arithmetic built into oracle/_ref) on a bounded sample
 and extrapolates to one proof.
 """
 import argparse
+import datetime
 import json
 import os
 import subprocess
@@ -36,7 +37,7 @@ FP_MUL_PER_G1_MADD = 10        # XYZZ mixed addition: 8M + 2S
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--log-m", type=int, default=20)
@@ -63,15 +64,19 @@ class Clocks:
     def start(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+
+    def mark(self, which):
+        """wall-clock bounds of the timed region ("begin" / "end")"""
+        setattr(self, which, datetime.datetime.now())
 
     def stop(self):
         if not self.proc:
@@ -84,9 +89,18 @@ class Clocks:
         rows = []
         for line in open(self.path):
             f = [x.strip() for x in line.split(",")]
-            if len(f) >= 9:
-                rows.append(f)
+            if len(f) < 10:
+                continue
+            try:
+                ts = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f")
+            except ValueError:
+                continue
+            rows.append((ts, f[1:]))
         os.unlink(self.path)
+        lo, hi = getattr(self, "begin", None), getattr(self, "end", None)
+        inside = [f for ts, f in rows if lo and hi and lo <= ts <= hi]
+        window = "timed region" if inside else "whole run (no sample fell inside the timed region)"
+        rows = inside or [f for _, f in rows]
         if not rows:
             return None
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
@@ -98,7 +112,7 @@ class Clocks:
                     reasons.add(n)
         return {"sm_mhz": float(np.median(sm)) if sm else None,
                 "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
-                "reasons": sorted(reasons), "samples": len(rows)}
+                "reasons": sorted(reasons), "samples": len(rows), "window": window}
 
 
 # --------------------------------------------------------------- CPU side
@@ -394,13 +408,13 @@ def main():
     def step(i, z):
         prover.prove(z, rs[i, 0], rs[i, 1], proof=proofs[i])
 
+    clocks = Clocks(local)
+    clocks.start()          # sampling starts during the warm-up
     for i in range(args.warmup):
         step(i, wits[i % nw])
     torch.cuda.synchronize()
 
     # ---------------- timed: device-resident inputs ----------------
-    clocks = Clocks(local)
-    clocks.start()
     _capi.trace_reset()
     _capi.trace_enable(True)
     if dist:
@@ -409,6 +423,7 @@ def main():
     launches0 = _capi.launch_count()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks.mark("begin")
     e0.record()
     for k in range(args.steps):
         ev[k][0].record()
@@ -416,6 +431,7 @@ def main():
         ev[k][1].record()
     e1.record()
     torch.cuda.synchronize()
+    clocks.mark("end")
     launches = _capi.launch_count() - launches0
     _capi.trace_enable(False)
     ms_total = e0.elapsed_time(e1)

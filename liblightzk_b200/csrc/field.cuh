@@ -6,14 +6,11 @@
 // mont_t<254,...> (include/device-arith/field/mont_t.cuh:47), so host arrays
 // cross the C-ABI unchanged.
 //
-// Multiplication is coarsely-integrated operand scanning over 32-bit limbs:
-// for every limb b_i of the multiplier, one carry chain of mad.lo and one of
-// mad.hi add a*b_i into a 9-limb accumulator, then m = t0 * (-p^-1 mod 2^32)
-// and two more chains add m*p, after which the accumulator shifts one limb.
-// Both moduli are below 2^254, so with inputs < p the accumulator stays
-// below 2^288 (9 limbs, no tenth carry) and ends below 2p; one conditional
-// subtraction makes every result canonical (< p), which keeps equality and
-// zero tests exact.
+// Multiplication is coarsely-integrated operand scanning over 32-bit limbs
+// (mont_mul_core); the result ends below 2p and one conditional subtraction
+// makes every result canonical (< p), which keeps equality and zero tests
+// exact.  Conversion out of Montgomery form uses explicit mad.lo / mad.hi
+// carry chains (red_row).
 #pragma once
 #include <cstdint>
 
@@ -149,30 +146,6 @@ __device__ __forceinline__ Fp<P> neg(const Fp<P>& a)
 
 template <class P> __device__ __forceinline__ Fp<P> dbl(const Fp<P>& a) { return add(a, a); }
 
-// One CIOS row: t[0..8] += a[0..7] * b   (t8 = 0 on entry)
-__device__ __forceinline__ void mac_row(uint32_t t[9], const uint32_t a[8], uint32_t b)
-{
-    asm("mad.lo.cc.u32  %0, %9,  %17, %0;\n\t"
-        "madc.lo.cc.u32 %1, %10, %17, %1;\n\t"
-        "madc.lo.cc.u32 %2, %11, %17, %2;\n\t"
-        "madc.lo.cc.u32 %3, %12, %17, %3;\n\t"
-        "madc.lo.cc.u32 %4, %13, %17, %4;\n\t"
-        "madc.lo.cc.u32 %5, %14, %17, %5;\n\t"
-        "madc.lo.cc.u32 %6, %15, %17, %6;\n\t"
-        "madc.lo.cc.u32 %7, %16, %17, %7;\n\t"
-        "addc.u32       %8, %8,  0;\n\t"
-        "mad.hi.cc.u32  %1, %9,  %17, %1;\n\t"
-        "madc.hi.cc.u32 %2, %10, %17, %2;\n\t"
-        "madc.hi.cc.u32 %3, %11, %17, %3;\n\t"
-        "madc.hi.cc.u32 %4, %12, %17, %4;\n\t"
-        "madc.hi.cc.u32 %5, %13, %17, %5;\n\t"
-        "madc.hi.cc.u32 %6, %14, %17, %6;\n\t"
-        "madc.hi.cc.u32 %7, %15, %17, %7;\n\t"
-        "madc.hi.u32    %8, %16, %17, %8;"
-        : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5]), "+r"(t[6]), "+r"(t[7]), "+r"(t[8])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]), "r"(b));
-}
-
 // One reduction row: m = t0 * INV; t += m * p; t >>= 32 (limb shift done by caller)
 template <class P>
 __device__ __forceinline__ void red_row(uint32_t t[9])
@@ -221,18 +194,48 @@ __device__ __forceinline__ Fp<P> final_sub(const uint32_t t[8])
     return r;
 }
 
+// Montgomery product core, t = a*b*2^-256 (t < 2p), for a, b < p.
+//
+// Operand scanning with the product row and the reduction row interleaved
+// limb by limb (CIOS), each step a 32x32+32+32-bit multiply-add into 64 bits:
+//   (A, t_j)     = t_j + a_j*b_i + A
+//   (C, t_{j-1}) = t_j + m*p_j + C
+// Because the top limb of p is below 2^31 - 1 (both BN254 moduli start
+// 0x30644e72), the accumulator never needs a ninth limb: after each row
+// t_7 = A + C fits in 32 bits (the "no-carry" condition of Montgomery
+// multiplication for moduli with a spare top bit).  Written over 64-bit
+// integers, the compiler maps each step to one wide multiply-add
+// (IMAD.WIDE.U32) and a short add, which issues fewer multiplier-pipe
+// instructions than separate mad.lo / mad.hi carry chains.
+template <class P>
+__host__ __device__ __forceinline__ void mont_mul_core(uint32_t t[8], const uint32_t a[8], const uint32_t b[8])
+{
+    _Pragma("unroll") for (int i = 0; i < 8; i++) t[i] = 0;
+    _Pragma("unroll") for (int i = 0; i < 8; i++) {
+        uint64_t s = (uint64_t)a[0] * b[i] + t[0];
+        uint32_t A = (uint32_t)(s >> 32);
+        t[0] = (uint32_t)s;
+        uint32_t m = t[0] * P::INV;
+        uint64_t u = (uint64_t)m * P::p(0) + t[0];
+        uint32_t C = (uint32_t)(u >> 32);
+        _Pragma("unroll") for (int j = 1; j < 8; j++) {
+            s = (uint64_t)a[j] * b[i] + t[j] + A;
+            A = (uint32_t)(s >> 32);
+            t[j] = (uint32_t)s;
+            u = (uint64_t)m * P::p(j) + t[j] + C;
+            C = (uint32_t)(u >> 32);
+            t[j - 1] = (uint32_t)u;
+        }
+        t[7] = C + A;
+    }
+}
+
 // Montgomery product a*b*2^-256 mod p
 template <class P>
 __device__ __forceinline__ Fp<P> mul(const Fp<P>& a, const Fp<P>& b)
 {
-    uint32_t t[9];
-    _Pragma("unroll") for (int i = 0; i < 9; i++) t[i] = 0;
-    _Pragma("unroll") for (int i = 0; i < 8; i++) {
-        mac_row(t, a.v, b.v[i]);
-        red_row<P>(t);
-        _Pragma("unroll") for (int j = 0; j < 8; j++) t[j] = t[j + 1];
-        t[8] = 0;
-    }
+    uint32_t t[8];
+    mont_mul_core<P>(t, a.v, b.v);
     return final_sub<P>(t);
 }
 
