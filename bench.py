@@ -44,8 +44,10 @@ def parse():
     ap.add_argument("--mode", choices=["standard", "reference"], default="standard")
     ap.add_argument("--window", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", choices=["prove", "msm-g1", "msm-g2", "ntt", "batch", "serve"], default="prove",
-                    help="prove = the benchmark; the others run one operator at --log-n for profiling")
+    ap.add_argument("--case", choices=["prove", "msm-g1", "msm-g2", "ntt", "batch", "serve", "reference-gpu"],
+                    default="prove",
+                    help="prove = the benchmark; msm-g1/msm-g2/ntt run one operator at --log-n for profiling; "
+                         "reference-gpu times the reference's own GPU programs (built by make -C oracle refgpu)")
     ap.add_argument("--log-n", type=int, default=20)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--inflight", type=int, default=4)
@@ -196,6 +198,46 @@ def run_reference_arm(args, rank, world):
 
 
 # --------------------------------------------------------------- GPU side
+def run_reference_gpu_case(args):
+    """The reference's own GPU path on this GPU, as its test programs run it:
+    oracle/_ref/groth16_gpu is test/groth16.cu (Groth16_BN254 with
+    MatMul_p_100: 2^20 constraints, Setup(12) then one Prove, whose phase
+    timers groth16.cuh:157-217 print wall times around synchronised
+    launches) and oracle/_ref/msm_check_gpu is test/msm-check.cu (G1 MSM
+    2^20, c = 12, timer msm-check.cu:38-41).  Both are the unmodified
+    reference sources compiled for sm_100a by oracle/Makefile.  Prints one
+    JSON line; the reference's inputs are its own unseeded random ones."""
+    import re
+    import subprocess
+    exe = {k: os.path.join(ROOT, "oracle", "_ref", k) for k in ("groth16_gpu", "msm_check_gpu")}
+    missing = [k for k, v in exe.items() if not os.path.exists(v)]
+    if missing:
+        print(json.dumps({"case": "reference-gpu", "unavailable": f"not built: {', '.join(missing)} "
+                          "(make -C oracle refgpu needs the reference tree)"}), flush=True)
+        return
+    env = dict(os.environ, CUDA_MODULE_LOADING="EAGER")
+    timing = re.compile(r"\[Timing\]\S*\s+(.*?) in: ([0-9.]+) seconds")
+
+    def run(path, timeout):
+        p = subprocess.run([path], env=env, capture_output=True, text=True, timeout=timeout)
+        if p.returncode != 0:
+            raise RuntimeError(f"{os.path.basename(path)} exited {p.returncode}: {p.stdout[-400:]}{p.stderr[-400:]}")
+        return [(m.group(1), float(m.group(2)) * 1e3) for m in timing.finditer(p.stdout)], p.stdout
+
+    msm_t, msm_out = run(exe["msm_check_gpu"], 900)
+    # timers in order: key generation, the MSM, the CPU check (msm-check.cu:31,41,55)
+    g1_ms = msm_t[1][1] if len(msm_t) >= 2 else None
+    g16_t, _ = run(exe["groth16_gpu"], 1500)
+    phases = {k: v for k, v in g16_t if k.startswith("Phase")}
+    prove_ms = sum(phases.values())
+    print(json.dumps({"case": "reference-gpu", "impl": "reference (its own GPU code on this GPU)",
+                      "workload": "groth16_prove_2^20 (MatMul_p_100: M = 2^20, N = 1030000)",
+                      "prove_ms": prove_ms, "proofs_per_s": 1e3 / prove_ms if prove_ms else None,
+                      "phases_ms": phases, "setup_ms": {k: v for k, v in g16_t if not k.startswith("Phase")},
+                      "g1_msm_2e20_ms": g1_ms, "g1_msm_window_bits": 12,
+                      "msm_check_ok": "Everything is OK!" in msm_out}), flush=True)
+
+
 def run_batch_case(args):
     """the batched-operator workload (64 G1 MSMs of 2^10..2^20 points and 32
     NTTs of 2^12..2^22 elements): one batch plan replayed as a CUDA graph,
@@ -336,11 +378,13 @@ def run_case(args):
     """one operator at 2^log_n, `reps` times, for profiling (prints ms)"""
     import torch
 
-    from liblightzk_b200 import msm, ntt, synth
+    from liblightzk_b200 import _capi, msm, ntt, synth
     if args.case == "batch":
         return run_batch_case(args)
     if args.case == "serve":
         return run_serve_case(args)
+    if args.case == "reference-gpu":
+        return run_reference_gpu_case(args)
     n = 1 << args.log_n
     sc = synth.random_fr(n, 5, 77)
     out = []
@@ -355,14 +399,25 @@ def run_case(args):
     else:
         ntt.prepare(args.log_n)
         fn = lambda: ntt.ntt(sc, args.log_n, ntt.COSET_FORWARD)  # noqa: E731
-    for _ in range(args.reps):
+    stages = {}
+    for r in range(args.reps):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        last = r == args.reps - 1
+        if last:     # per-stage device times of the last repetition
+            _capi.trace_reset()
+            _capi.trace_enable(True)
         a.record()
         fn()
         b.record()
         torch.cuda.synchronize()
         out.append(a.elapsed_time(b))
-    print(json.dumps({"case": args.case, "log_n": args.log_n, "window": args.window, "ms": out}), flush=True)
+        if last:
+            _capi.trace_enable(False)
+            if args.case in ("msm-g1", "msm-g2"):
+                for st in ("sort", "accumulate", "fixup", "reduce"):
+                    stages[st] = _capi.trace_get(f"msm_g{g}_{st}")[0]
+    print(json.dumps({"case": args.case, "log_n": args.log_n, "window": args.window, "ms": out,
+                      "stages_ms": stages}), flush=True)
 
 
 def main():
@@ -466,6 +521,7 @@ def main():
 
     # ---------------- G1 MSM at 2^20 (precomputed table, as msm-check.cu) ----------------
     g1_ms = g1_plain_ms = None
+    iso_ms = iso_n = iso_pts = 0
     if rank == 0:
         n = 1 << 20
         sc = synth.random_fr(n, 5, 77, device=dev)
@@ -477,12 +533,18 @@ def main():
         times = []
         for it in range(8):
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            if it == 3:     # accumulation-kernel times of the measured repetitions, alone on the GPU
+                _capi.trace_reset()
+                _capi.trace_enable(True)
             a.record()
             msm.msm_precomputed(1, sc, table, c, W, n, workspace=ws)
             b.record()
             torch.cuda.synchronize()
             if it >= 3:
                 times.append(a.elapsed_time(b))
+        _capi.trace_enable(False)
+        iso_ms, iso_n = _capi.trace_get("msm_g1_accumulate")
+        iso_pts = n
         g1_ms = float(np.median(times))
         del table
         times = []
@@ -520,6 +582,15 @@ def main():
         except Exception:
             traffic = None
 
+    iso_line = None
+    if iso_n:
+        iso_alg = iso_pts * W * FP_MUL_PER_G1_MADD * IMAD_PER_FP_MUL
+        iso_avg = iso_ms / iso_n
+        iso_line = {"workload": f"G1 MSM 2^{int(np.log2(iso_pts))} alone", "avg_launch_ms": iso_avg,
+                    "launches": iso_n, "achieved": iso_alg / (iso_avg * 1e-3) / 1e12,
+                    "frac": iso_alg / (iso_avg * 1e-3) / imad_peak,
+                    "traffic_bytes": traffic * iso_pts / (avg_pts if avg_pts else 1) if traffic else None}
+
     proofs_s = world * args.steps / (ms_total * 1e-3)
     line = {
         "metric": METRIC, "value": proofs_s, "unit": "proofs/s", "n_gpus": world, "steps": args.steps,
@@ -540,7 +611,11 @@ def main():
                      "unit": "T IMAD/s", "frac": (achieved / imad_peak) if achieved else None,
                      "traffic": traffic, "peak_source": "measured (lzk_probe_imad_rate, mad.lo/madc.hi chains)",
                      "algorithmic_imad_per_launch": alg_imad, "avg_launch_ms": acc_avg_ms,
-                     "launches": acc_n},
+                     "launches": acc_n,
+                     "timing": "CUDA events around each launch inside the timed proofs; the four G1 MSMs "
+                               "of a proof overlap on two streams, so a launch shares the GPU",
+                     "isolated": iso_line},
+        # sums of per-call device times; calls on different streams overlap
         "breakdown_ms_per_proof": {"msm_g1": msm1_ms / args.steps, "msm_g2": msm2_ms / args.steps,
                                    "msm_g1_accumulate": acc_ms / args.steps,
                                    "msm_g2_accumulate": acc2_ms / args.steps},

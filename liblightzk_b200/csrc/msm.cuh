@@ -340,7 +340,9 @@ int run_msm(const Fr* scalars, const void* bases, size_t n, Jac<typename Gp::F>*
 
     uint32_t* bsums = reinterpret_cast<uint32_t*>(base + p.o_scan);
     uint32_t* large = reinterpret_cast<uint32_t*>(base + p.o_large);
+    void* tr_sort = trace_begin(sizeof(F) == 32 ? "msm_g1_sort" : "msm_g2_sort", st);
     LZK_TRY(msm_sort(p, scalars, cnt, off, ent, bsums, st));
+    trace_end(tr_sort, st);
     void* tr = trace_begin(sizeof(F) == 32 ? "msm_g1_accumulate" : "msm_g2_accumulate", st);
     {
         unsigned g = grid_for(p.chunks, 128);
@@ -352,15 +354,18 @@ int run_msm(const Fr* scalars, const void* bases, size_t n, Jac<typename Gp::F>*
         }
     }
     trace_end(tr, st);
+    void* tr_fix = trace_begin(sizeof(F) == 32 ? "msm_g1_fixup" : "msm_g2_fixup", st);
     LZK_CUDA(cudaMemsetAsync(large, 0, sizeof(uint32_t), st));
     k_fixup<F><<<grid_for(p.B, 256, 148 * 8), 256, 0, st>>>(off, p.B, bsum, head, tail, large); note_launch();
     {
         constexpr unsigned fx_threads = 32768 / sizeof(X);   // 32 KB of shared memory
         k_fixup_large<F><<<148 * 2, fx_threads, fx_threads * sizeof(X), st>>>(off, bsum, head, tail, large); note_launch();
     }
+    trace_end(tr_fix, st);
     LZK_TRY(launch_status());
 
     // weighted sums per bucket set
+    void* tr_red = trace_begin(sizeof(F) == 32 ? "msm_g1_reduce" : "msm_g2_reduce", st);
     const X* inR = bsum; const X* inA = nullptr; const uint32_t* offp = off;
     uint32_t m = p.nb, logM = 0, base1 = 1, pp = 0;
     X* resA = nullptr;
@@ -378,6 +383,7 @@ int run_msm(const Fr* scalars, const void* bases, size_t n, Jac<typename Gp::F>*
         if (m == 1) break;
     }
     k_finish<F><<<1, 32, 0, st>>>(resA, p.wb, c, out); note_launch();
+    trace_end(tr_red, st);
     trace_end(tr_all, st);
     return launch_status();
 }
