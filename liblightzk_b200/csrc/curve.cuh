@@ -32,12 +32,60 @@ __device__ __forceinline__ Fq2 add(const Fq2& a, const Fq2& b) { return {add(a.c
 __device__ __forceinline__ Fq2 sub(const Fq2& a, const Fq2& b) { return {sub(a.c0, b.c0), sub(a.c1, b.c1)}; }
 __device__ __forceinline__ Fq2 neg(const Fq2& a) { return {neg(a.c0), neg(a.c1)}; }
 __device__ __forceinline__ Fq2 dbl(const Fq2& a) { return {dbl(a.c0), dbl(a.c1)}; }
-// Karatsuba: 3 Fq products
+// p^2 (Fq), 16 limbs
+__host__ __device__ constexpr uint32_t fq_p2(int i)
+{
+    return i == 0 ? 0x275d69b1u : i == 1 ? 0x3b5458a2u : i == 2 ? 0x09eac101u : i == 3 ? 0xa602072du
+         : i == 4 ? 0x6d96cadcu : i == 5 ? 0x4a50189cu : i == 6 ? 0x7a1242c8u : i == 7 ? 0x04689e95u
+         : i == 8 ? 0x34c6b38du : i == 9 ? 0x26edfa5cu : i == 10 ? 0x16375606u : i == 11 ? 0xb00b8551u
+         : i == 12 ? 0x0348d21cu : i == 13 ? 0x599a6f7cu : i == 14 ? 0x763cbf9cu : 0x0925c4b8u;
+}
+
+// Karatsuba with lazy reduction: the three 512-bit products stay unreduced,
+//   c0 = a0 b0 + p^2 - a1 b1,   c1 = (a0 + a1)(b0 + b1) - a0 b0 - a1 b1,
+// both in (0, 2p^2) < p 2^256, and only c0 and c1 are reduced (two
+// Montgomery reductions instead of three).  The operand sums are < 2p and
+// fit 8 limbs unreduced.  The reductions give (a0 b0 - a1 b1) R^-1 and
+// (a0 b1 + a1 b0) R^-1 mod p below 2p, so after the final conditional
+// subtraction the result is the canonical value that three separately
+// reduced products give.
+__host__ __device__ __forceinline__ void fq2_mul_lazy(uint32_t c0[8], uint32_t c1[8], const uint32_t a0[8],
+                                                      const uint32_t a1[8], const uint32_t b0[8], const uint32_t b1[8])
+{
+    uint32_t t0[16], t1[16], t2[16], sa[8], sb[8];
+    mul_wide(t0, a0, b0);
+    mul_wide(t1, a1, b1);
+    uint32_t ca = 0, cb = 0;
+    _Pragma("unroll") for (int k = 0; k < 8; k++) {
+        uint64_t x = (uint64_t)a0[k] + a1[k] + ca;
+        sa[k] = (uint32_t)x; ca = (uint32_t)(x >> 32);
+        uint64_t y = (uint64_t)b0[k] + b1[k] + cb;
+        sb[k] = (uint32_t)y; cb = (uint32_t)(y >> 32);
+    }
+    mul_wide(t2, sa, sb);
+    // t2 -= t0 + t1 ; t0 = t0 + p^2 - t1
+    uint32_t b2 = 0, c = 0, b0r = 0;
+    _Pragma("unroll") for (int k = 0; k < 16; k++) {
+        uint64_t d = (uint64_t)t2[k] - t0[k] - t1[k] - b2;
+        t2[k] = (uint32_t)d;
+        b2 = (uint32_t)(0u - (uint32_t)(d >> 32));   // borrow 0, 1 or 2
+        uint64_t e = (uint64_t)t0[k] + fq_p2(k) + c;
+        c = (uint32_t)(e >> 32);
+        uint64_t f = (uint64_t)(uint32_t)e - t1[k] - b0r;
+        t0[k] = (uint32_t)f;
+        b0r = (uint32_t)(f >> 63);
+    }
+    uint32_t r0[8], r1[8];
+    redc_wide<FqP>(r0, t0);
+    redc_wide<FqP>(r1, t2);
+    _Pragma("unroll") for (int k = 0; k < 8; k++) { c0[k] = r0[k]; c1[k] = r1[k]; }
+}
+
 __device__ __forceinline__ Fq2 mul(const Fq2& a, const Fq2& b)
 {
-    Fq aa = mul(a.c0, b.c0), bb = mul(a.c1, b.c1);
-    Fq s = mul(add(a.c0, a.c1), add(b.c0, b.c1));
-    return {sub(aa, bb), sub(sub(s, aa), bb)};
+    uint32_t r0[8], r1[8];
+    fq2_mul_lazy(r0, r1, a.c0.v, a.c1.v, b.c0.v, b.c1.v);
+    return {final_sub<FqP>(r0), final_sub<FqP>(r1)};
 }
 // (a0 + a1 i)^2 = (a0+a1)(a0-a1) + 2 a0 a1 i: 2 Fq products
 __device__ __forceinline__ Fq2 sqr(const Fq2& a)
@@ -55,9 +103,9 @@ static __device__ __noinline__ Fq2 inverse(const Fq2& a)
 // Fq2 products built from them.
 __device__ __forceinline__ Fq cmul(const Fq& a, const Fq& b) { return mul_call(a, b); }
 __device__ __forceinline__ Fq csqr(const Fq& a) { return mul_call(a, a); }
-// One out-of-line body per Fq2 product (and square): its three (two) Fq
-// products are inlined there, so they interleave, and the call boundary
-// moves two Fq2 operands once instead of once per Fq product.
+// One out-of-line body per Fq2 product (and square): its limb products are
+// inlined there, so they interleave, and the call boundary moves two Fq2
+// operands once instead of once per Fq product.
 static __device__ __noinline__ Fq2 fq2_mul_call(const Fq2 a, const Fq2 b) { return mul(a, b); }
 static __device__ __noinline__ Fq2 fq2_sqr_call(const Fq2 a) { return sqr(a); }
 __device__ __forceinline__ Fq2 cmul(const Fq2& a, const Fq2& b) { return fq2_mul_call(a, b); }

@@ -230,6 +230,45 @@ __host__ __device__ __forceinline__ void mont_mul_core(uint32_t t[8], const uint
     }
 }
 
+// Full 512-bit product t = a*b of two 8-limb integers (operand scanning,
+// one 32x32+32+32-bit multiply-add into 64 bits per limb pair).
+__host__ __device__ __forceinline__ void mul_wide(uint32_t t[16], const uint32_t a[8], const uint32_t b[8])
+{
+    _Pragma("unroll") for (int i = 0; i < 16; i++) t[i] = 0;
+    _Pragma("unroll") for (int i = 0; i < 8; i++) {
+        uint32_t C = 0;
+        _Pragma("unroll") for (int j = 0; j < 8; j++) {
+            uint64_t s = (uint64_t)a[j] * b[i] + t[i + j] + C;
+            t[i + j] = (uint32_t)s;
+            C = (uint32_t)(s >> 32);
+        }
+        t[i + 8] = C;
+    }
+}
+
+// Montgomery reduction r = t*2^-256 (r < 2p) of a 512-bit t < p*2^256,
+// row by row (separated operand scanning); the carry out of each row's top
+// limb is added one limb higher in the next row.  t is consumed.
+template <class P>
+__host__ __device__ __forceinline__ void redc_wide(uint32_t r[8], uint32_t t[16])
+{
+    uint32_t top = 0;
+    _Pragma("unroll") for (int i = 0; i < 8; i++) {
+        uint32_t m = t[i] * P::INV;
+        uint64_t s = (uint64_t)m * P::p(0) + t[i];
+        uint32_t C = (uint32_t)(s >> 32);
+        _Pragma("unroll") for (int j = 1; j < 8; j++) {
+            s = (uint64_t)m * P::p(j) + t[i + j] + C;
+            t[i + j] = (uint32_t)s;
+            C = (uint32_t)(s >> 32);
+        }
+        uint64_t u = (uint64_t)t[i + 8] + C + top;
+        t[i + 8] = (uint32_t)u;
+        top = (uint32_t)(u >> 32);
+    }
+    _Pragma("unroll") for (int j = 0; j < 8; j++) r[j] = t[8 + j];
+}
+
 // Montgomery product a*b*2^-256 mod p
 template <class P>
 __device__ __forceinline__ Fp<P> mul(const Fp<P>& a, const Fp<P>& b)
