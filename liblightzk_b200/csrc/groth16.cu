@@ -157,13 +157,14 @@ void ctx_destroy(ProveCtx* x)
 {
     if (!x) return;
     for (auto w : x->ws) if (w) cudaFree(w);
-    void* misc[] = {x->x, x->g1res, x->g2res, x->sm1, x->sm2, x->z, x->proof};
+    void* misc[] = {x->x, x->g1res, x->g2res, x->sm1, x->sm2, x->z, x->proof,
+                    x->zs_cnt, x->zs_off, x->zs_ent, x->zs_bsums};
     for (auto m : misc) if (m) cudaFree(m);
     if (x->proof_host) cudaFreeHost(x->proof_host);
     if (x->ev_done) cudaEventDestroy(x->ev_done);
     cudaStream_t sts[] = {x->s0, x->s1, x->s2, x->s3};
     for (auto t : sts) if (t) cudaStreamDestroy(t);
-    cudaEvent_t evs[] = {x->ev_fork, x->ev_b1, x->ev_s1, x->ev_s2, x->ev_s3};
+    cudaEvent_t evs[] = {x->ev_fork, x->ev_b1, x->ev_s1, x->ev_s2, x->ev_s3, x->ev_sorted};
     for (auto e : evs) if (e) cudaEventDestroy(e);
     delete x;
 }
@@ -193,6 +194,14 @@ int ctx_create(const lzk_prover* p, bool serving, ProveCtx** out)
             rc = dalloc(&x->bytes, reinterpret_cast<char**>(&x->ws[i]), x->wsb[i]);
         }
         if (rc) break;
+        {
+            // the A, B1 and B2 tables all have level stride n_vars
+            SortWords w = msm_sort_words(p->n_vars, p->c, p->n_vars);
+            if ((rc = dalloc(&x->bytes, &x->zs_cnt, w.cnt))) break;
+            if ((rc = dalloc(&x->bytes, &x->zs_off, w.off))) break;
+            if ((rc = dalloc(&x->bytes, &x->zs_ent, w.ent))) break;
+            if ((rc = dalloc(&x->bytes, &x->zs_bsums, w.bsums))) break;
+        }
         if (serving) {
             if ((rc = dalloc(&x->bytes, &x->z, p->n_vars))) break;
             if ((rc = dalloc(&x->bytes, &x->proof, 1))) break;
@@ -202,7 +211,7 @@ int ctx_create(const lzk_prover* p, bool serving, ProveCtx** out)
         }
         cudaStream_t* sts[] = {&x->s1, &x->s2, &x->s3};
         for (auto t : sts) if (cudaStreamCreateWithFlags(t, cudaStreamNonBlocking) != cudaSuccess) rc = LZK_EDEVICE;
-        cudaEvent_t* evs[] = {&x->ev_fork, &x->ev_b1, &x->ev_s1, &x->ev_s2, &x->ev_s3};
+        cudaEvent_t* evs[] = {&x->ev_fork, &x->ev_b1, &x->ev_s1, &x->ev_s2, &x->ev_s3, &x->ev_sorted};
         for (auto e : evs) if (cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess) rc = LZK_EDEVICE;
     } while (0);
     if (rc != LZK_OK) { cudaGetLastError(); ctx_destroy(x); return rc; }
@@ -284,7 +293,7 @@ static int create(const lzk_groth16_circuit* c, const lzk_groth16_pk* pk, int mo
 }
 
 static int msm_tab1(const lzk_prover* p, ProveCtx* x, int q, const Fr* scal, size_t n, Jac<Fq>* out, int wsi,
-                    cudaStream_t st)
+                    cudaStream_t st, bool presorted = false)
 {
     lzk_msm_cfg cfg{};
     cfg.window_bits = p->c;
@@ -293,6 +302,7 @@ static int msm_tab1(const lzk_prover* p, ProveCtx* x, int q, const Fr* scal, siz
     cfg.level_stride = p->tn[q];
     cfg.workspace = x->ws[wsi];
     cfg.workspace_bytes = x->wsb[wsi];
+    if (presorted) return msm_g1_presorted(scal, p->tab[q], n, out, &cfg, st, x->zs_off, x->zs_ent);
     return lzk_msm_g1(reinterpret_cast<const lzk_fr_t*>(scal), reinterpret_cast<const lzk_g1_affine_t*>(p->tab[q]), n,
                       reinterpret_cast<lzk_g1_t*>(out), &cfg, st);
 }
@@ -311,6 +321,12 @@ int prove_ctx(const lzk_prover* p, ProveCtx* x, const Fr* z, const lzk_fr_t* r, 
     // s3: fixed-base products
     k_fixed_products<<<1, 32, 0, x->s3>>>(p->comb1, p->comb2, rs, ss, x->sm1, x->sm2); note_launch();
 
+    // s1: one digit sort of z for the A, B1 and B2 MSMs (same scalars, same
+    // window width, tables of the same level stride n_vars)
+    LZK_TRY(msm_sort_scalars(z, p->n_vars, p->c, p->n_vars, x->zs_cnt, x->zs_off, x->zs_ent, x->zs_bsums, x->s1));
+    LZK_CUDA(cudaEventRecord(x->ev_sorted, x->s1));
+    LZK_CUDA(cudaStreamWaitEvent(x->s2, x->ev_sorted, 0));
+
     // s2: the G2 MSM
     {
         lzk_msm_cfg cfg{};
@@ -320,14 +336,13 @@ int prove_ctx(const lzk_prover* p, ProveCtx* x, const Fr* z, const lzk_fr_t* r, 
         cfg.level_stride = p->tn2;
         cfg.workspace = x->ws[2];
         cfg.workspace_bytes = x->wsb[2];
-        LZK_TRY(lzk_msm_g2(reinterpret_cast<const lzk_fr_t*>(z), reinterpret_cast<const lzk_g2_affine_t*>(p->tab2),
-                           p->n_vars, reinterpret_cast<lzk_g2_t*>(x->g2res), &cfg, x->s2));
+        LZK_TRY(msm_g2_presorted(z, p->tab2, p->n_vars, x->g2res, &cfg, x->s2, x->zs_off, x->zs_ent));
     }
     LZK_CUDA(cudaEventRecord(x->ev_s2, x->s2));
 
     // s1: A, B1 and L MSMs; s3 picks up A and B1 for s*A and r*B1
-    LZK_TRY(msm_tab1(p, x, 0, z, p->n_vars, x->g1res + 0, 1, x->s1));
-    LZK_TRY(msm_tab1(p, x, 1, z, p->n_vars, x->g1res + 1, 1, x->s1));
+    LZK_TRY(msm_tab1(p, x, 0, z, p->n_vars, x->g1res + 0, 1, x->s1, true));
+    LZK_TRY(msm_tab1(p, x, 1, z, p->n_vars, x->g1res + 1, 1, x->s1, true));
     LZK_CUDA(cudaEventRecord(x->ev_b1, x->s1));
     LZK_CUDA(cudaStreamWaitEvent(x->s3, x->ev_b1, 0));
     k_dep_products<<<1, 32, 0, x->s3>>>(x->g1res, rs, ss, x->sm1); note_launch();

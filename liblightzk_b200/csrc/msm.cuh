@@ -64,6 +64,20 @@ inline void plan_msm(MsmPlan& p, size_t n, uint32_t c, bool shared, size_t strid
 int msm_sort(const MsmPlan& p, const Fr* scalars, uint32_t* cnt, uint32_t* off, uint32_t* ent, uint32_t* bsums,
              cudaStream_t st);
 uint32_t msm_autotune(int group, size_t n, bool shared);
+
+// One digit sort shared by several shifted-table MSMs over the same scalars
+// (the Groth16 A, B1 and B2 queries all take the witness): sizes of its
+// buffers in 32-bit words, the sort itself, and the G1 / G2 MSMs that consume
+// it (msm_sort.cu, msm_g1.cu, msm_g2.cu).  The consumers must use the same
+// n, window width and table level stride as the sort.
+struct SortWords { size_t cnt, off, ent, bsums; };
+SortWords msm_sort_words(size_t n, uint32_t c, size_t stride);
+int msm_sort_scalars(const Fr* scalars, size_t n, uint32_t c, size_t stride, uint32_t* cnt, uint32_t* off,
+                     uint32_t* ent, uint32_t* bsums, cudaStream_t st);
+int msm_g1_presorted(const Fr* scalars, const void* table, size_t n, Jac<Fq>* out, const lzk_msm_cfg* cfg,
+                     cudaStream_t st, const uint32_t* off, const uint32_t* ent);
+int msm_g2_presorted(const Fr* scalars, const void* table, size_t n, Jac<Fq2>* out, const lzk_msm_cfg* cfg,
+                     cudaStream_t st, const uint32_t* off, const uint32_t* ent);
 // exclusive scan of cnt[0..B) into off[0..B], off[B] = total; bsums holds
 // (B + 4095) / 4096 + 1 words (msm_sort.cu)
 int scan_offsets(const uint32_t* cnt, uint32_t B, uint32_t* off, uint32_t* bsums, cudaStream_t st);
@@ -298,9 +312,13 @@ __global__ void k_write_inf(Jac<F>* out)
     if (gtid() == 0) st_elem(out, Jac<F>{F::zero(), F::one(), F::zero()});
 }
 
+// pre_off / pre_ent: bucket offsets and sorted entries of these scalars made
+// earlier by msm_sort for the same n, window width and table stride (MSMs
+// over the same scalars share one sort); null = sort here.
 template <class Gp>
 int run_msm(const Fr* scalars, const void* bases, size_t n, Jac<typename Gp::F>* out,
-                   const lzk_msm_cfg* cfg, cudaStream_t st, uint32_t c_auto)
+                   const lzk_msm_cfg* cfg, cudaStream_t st, uint32_t c_auto,
+                   const uint32_t* pre_off = nullptr, const uint32_t* pre_ent = nullptr)
 {
     using F = typename Gp::F;
     using X = XYZZ<F>;
@@ -330,8 +348,10 @@ int run_msm(const Fr* scalars, const void* bases, size_t n, Jac<typename Gp::F>*
     LZK_TRY(ws.acquire(p.bytes, cfg ? cfg->workspace : nullptr, cfg ? cfg->workspace_bytes : 0, st));
     char* base = ws.base;
     uint32_t* cnt = reinterpret_cast<uint32_t*>(base + p.o_cnt);
-    uint32_t* off = reinterpret_cast<uint32_t*>(base + p.o_off);
-    uint32_t* ent = reinterpret_cast<uint32_t*>(base + p.o_ent);
+    uint32_t* off_ws = reinterpret_cast<uint32_t*>(base + p.o_off);
+    uint32_t* ent_ws = reinterpret_cast<uint32_t*>(base + p.o_ent);
+    const uint32_t* off = pre_off ? pre_off : off_ws;
+    const uint32_t* ent = pre_ent ? pre_ent : ent_ws;
     X* bsum = reinterpret_cast<X*>(base + p.o_bsum);
     X* head = reinterpret_cast<X*>(base + p.o_head);
     X* tail = reinterpret_cast<X*>(base + p.o_tail);
@@ -340,9 +360,11 @@ int run_msm(const Fr* scalars, const void* bases, size_t n, Jac<typename Gp::F>*
 
     uint32_t* bsums = reinterpret_cast<uint32_t*>(base + p.o_scan);
     uint32_t* large = reinterpret_cast<uint32_t*>(base + p.o_large);
-    void* tr_sort = trace_begin(sizeof(F) == 32 ? "msm_g1_sort" : "msm_g2_sort", st);
-    LZK_TRY(msm_sort(p, scalars, cnt, off, ent, bsums, st));
-    trace_end(tr_sort, st);
+    if (!pre_off) {
+        void* tr_sort = trace_begin(sizeof(F) == 32 ? "msm_g1_sort" : "msm_g2_sort", st);
+        LZK_TRY(msm_sort(p, scalars, cnt, off_ws, ent_ws, bsums, st));
+        trace_end(tr_sort, st);
+    }
     void* tr = trace_begin(sizeof(F) == 32 ? "msm_g1_accumulate" : "msm_g2_accumulate", st);
     {
         unsigned g = grid_for(p.chunks, 128);

@@ -4,6 +4,15 @@
 
 using namespace lzk;
 
+namespace lzk {
+int msm_g2_presorted(const Fr* scalars, const void* table, size_t n, Jac<Fq2>* out, const lzk_msm_cfg* cfg,
+                     cudaStream_t st, const uint32_t* off, const uint32_t* ent)
+{
+    if (!cfg || !(cfg->flags & LZK_MSM_PRECOMPUTED) || !off || !ent) return LZK_EINVAL;
+    return run_msm<G2>(scalars, table, n, out, cfg, st, cfg->window_bits, off, ent);
+}
+}  // namespace lzk
+
 extern "C" {
 
 int lzk_msm_g2(const lzk_fr_t* scalars, const void* bases, size_t n, lzk_g2_t* out,

@@ -204,6 +204,25 @@ uint32_t msm_autotune(int group, size_t n, bool shared)
     return bc;
 }
 
+SortWords msm_sort_words(size_t n, uint32_t c, size_t stride)
+{
+    MsmPlan p;
+    plan_msm<G1>(p, n, c, true, stride);
+    return SortWords{p.B, (size_t)p.B + 1, p.max_entries ? p.max_entries : 1, (p.B + 4095) / 4096 + 1};
+}
+
+int msm_sort_scalars(const Fr* scalars, size_t n, uint32_t c, size_t stride, uint32_t* cnt, uint32_t* off,
+                     uint32_t* ent, uint32_t* bsums, cudaStream_t st)
+{
+    if (!n || c < 2 || c > 24 || stride < n) return LZK_EINVAL;
+    MsmPlan p;
+    plan_msm<G1>(p, n, c, true, stride);
+    void* tr = trace_begin("msm_shared_sort", st);
+    int rc = msm_sort(p, scalars, cnt, off, ent, bsums, st);
+    trace_end(tr, st);
+    return rc;
+}
+
 }  // namespace lzk
 
 using namespace lzk;

@@ -18,12 +18,15 @@ struct ProveCtx {
     XYZZ<Fq2>* sm2 = nullptr;         // s d2
     void* ws[3] = {nullptr, nullptr, nullptr};
     size_t wsb[3] = {0, 0, 0};
+    // one digit sort of the witness, shared by the A, B1 and B2 MSMs
+    uint32_t *zs_cnt = nullptr, *zs_off = nullptr, *zs_ent = nullptr, *zs_bsums = nullptr;
     Fr* z = nullptr;                  // witness buffer (serving contexts only)
     lzk_groth16_proof* proof = nullptr;   // proof buffer (serving contexts only)
     lzk_groth16_proof* proof_host = nullptr;   // pinned copy target (serving contexts only)
     cudaEvent_t ev_done = nullptr;             // end of the proof on s0 (serving contexts only)
     cudaStream_t s0 = nullptr, s1 = nullptr, s2 = nullptr, s3 = nullptr;   // s0: serving contexts only
-    cudaEvent_t ev_fork = nullptr, ev_b1 = nullptr, ev_s1 = nullptr, ev_s2 = nullptr, ev_s3 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_b1 = nullptr, ev_s1 = nullptr, ev_s2 = nullptr, ev_s3 = nullptr,
+                ev_sorted = nullptr;
     size_t bytes = 0;
 };
 
