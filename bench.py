@@ -42,6 +42,10 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--log-m", type=int, default=20)
     ap.add_argument("--mode", choices=["standard", "reference"], default="standard")
+    ap.add_argument("--circuit", choices=["synthetic", "matmul"], default="synthetic",
+                    help="synthetic = the benchmark circuit (--log-m); matmul = the reference's own MatMul "
+                         "circuit (--matmul-p; p = 100 gives 2^20 constraints)")
+    ap.add_argument("--matmul-p", type=int, default=100)
     ap.add_argument("--window", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--case", choices=["prove", "msm-g1", "msm-g2", "ntt", "batch", "serve", "reference-gpu"],
@@ -443,11 +447,15 @@ def main():
 
     from liblightzk_b200 import _capi, device, groth16, msm, synth
     dev = f"cuda:{local}"
-    log_m = args.log_m
-    M = 1 << log_m
-
     # ---------------- setup (untimed) ----------------
-    circ = synth.Circuit(log_m, seed=1, device=dev)
+    if args.circuit == "matmul":
+        circ = synth.MatMulCircuit(args.matmul_p, device=dev)
+        workload = f"groth16_prove_matmul_p{args.matmul_p}"
+    else:
+        circ = synth.Circuit(args.log_m, seed=1, device=dev)
+        workload = f"groth16_prove_2^{args.log_m}"
+    log_m = circ.log_m
+    M = circ.M
     pk = synth.ProvingKey(circ, seed=7)
     mode = groth16.STANDARD if args.mode == "standard" else groth16.REFERENCE
     prover = groth16.Prover(circ, pk, mode=mode, window_bits=args.window)
@@ -597,7 +605,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32 limbs (Fr/Fq mod p, Montgomery)",
         "data": "synthetic (seeded R1CS, witness and proving key generated on the device)",
-        "config": {"workload": f"groth16_prove_2^{log_m}", "constraints": M, "variables": circ.n_vars,
+        "config": {"workload": workload, "constraints": M, "variables": circ.n_vars,
                    "public_inputs": circ.n_public, "prove_mode": args.mode, "msm_window_bits": args.window,
                    "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (GB-scale key tables)"},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),

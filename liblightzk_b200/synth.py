@@ -44,7 +44,9 @@ def fixed_base(group, k, stream=None):
 
 
 class Matrix:
-    """CSR matrix in device memory (uint32 indices, rows+1 offsets)."""
+    """CSR matrix in device memory: 4- or 8-byte indices (from col's dtype);
+    row_ptr with rows + 1 offsets, or the reference's rows offsets with the
+    last row ending at nnz."""
 
     def __init__(self, val, col, row_ptr, rows, cols):
         self.val, self.col, self.row_ptr = val, col, row_ptr
@@ -57,7 +59,10 @@ class Matrix:
     def host(self):
         """(val, col, row_ptr) as numpy uint64 arrays (row_ptr with rows+1 entries)"""
         from .device import to_host
-        return (to_host(self.val), to_host(self.col).astype(np.uint64), to_host(self.row_ptr).astype(np.uint64))
+        rp = to_host(self.row_ptr).astype(np.uint64)
+        if rp.shape[0] == self.rows:       # the reference's layout: the last row ends at nnz
+            rp = np.append(rp, np.uint64(self.nnz))
+        return (to_host(self.val), to_host(self.col).astype(np.uint64), rp)
 
 
 def _rows(rng, unit, avail, maxextra):
@@ -143,3 +148,65 @@ class ProvingKey:
         g2 = fixed_base(2, random_fr(2, seed, sid + 6, device=dev))
         self.alpha1, self.beta1, self.delta1 = g1[0], g1[1], g1[2]
         self.beta2, self.delta2 = g2[0], g2[1]
+
+
+def _next_pow2(x):
+    return 1 << max(0, int(x - 1).bit_length())
+
+
+class MatMulCircuit:
+    """The reference's benchmark circuit: the product Z = X Y of two p x p
+    matrices (xpu-spmat.cuh:33-65, Groth16 input scales MatMul_p_39 / 63 /
+    100 of groth16.cuh:11-46, i.e. 2^16, 2^18 and 2^20 constraints).
+
+    Variables: z_0 = 1, X (p^2), Y (p^2), Z (p^2), then the p^3 products
+    t_(i1 p^2 + i2 p + i3); the k = 3p^2 entries of X, Y and Z are the public
+    inputs.  Rows 0 .. p^3 - 1 are the products (A selects X, B selects Y,
+    C selects t), rows p^3 .. p^3 + p^2 - 1 the sums (A adds p products, B
+    is the constant 1, C selects Z), the remaining rows up to
+    M = next_pow2(p^3 + p^2) are empty; every coefficient is one.  The
+    matrices are built with the reference's layout: 8-byte column indices and
+    row offsets, `rows` = M offsets with the last row ending at nnz.  Unlike
+    the reference's random witness (groth16.cuh:128-132), witness() solves the
+    gates, so the instance is satisfied."""
+
+    def __init__(self, p, device="cuda"):
+        self.p = p
+        p2, p3 = p * p, p * p * p
+        self.M = M = _next_pow2(p3 + p2)
+        self.log_m = M.bit_length() - 1
+        self.n_public = 3 * p2
+        self.n_vars = 1 + 3 * p2 + p3
+        self.device = device
+        i = np.arange(p3, dtype=np.int64)
+        i1, i2, i3 = i // p2, (i % p2) // p, i % p
+        r = np.arange(p2, dtype=np.int64)
+        a_col = np.concatenate([1 + i2 * p + i1, (1 + 3 * p2 + np.arange(p)[None, :] * p2 + r[:, None]).reshape(-1)])
+        a_ptr = np.concatenate([np.arange(p3), p3 + p * r, np.full(M - p3 - p2, 2 * p3)])
+        b_col = np.concatenate([1 + p2 + i1 * p + i3, np.zeros(p2, np.int64)])
+        c_col = np.concatenate([1 + 3 * p2 + i, 1 + 2 * p2 + r])
+        bc_ptr = np.concatenate([np.arange(p3 + p2), np.full(M - p3 - p2, p3 + p2)])
+        one = torch.from_numpy(FR_ONE.view(np.int64)).to(device)
+        self.mats = []
+        for col, rp in ((a_col, a_ptr), (b_col, bc_ptr), (c_col, bc_ptr)):
+            val = one.repeat(col.shape[0], 1)
+            self.mats.append(Matrix(val, torch.from_numpy(col).to(device), torch.from_numpy(rp.astype(np.int64)).to(device),
+                                    M, self.n_vars))
+        self.A, self.B, self.C = self.mats
+
+    def witness(self, wseed):
+        """z_0 = 1, X and Y uniform (seeded), then the products and the sums
+        solved on the device (lzk_r1cs_solve)"""
+        import ctypes
+        p2, p3 = self.p * self.p, self.p ** 3
+        z = torch.zeros((self.n_vars, 4), dtype=torch.int64, device=self.device)
+        z[0] = torch.from_numpy(FR_ONE.view(np.int64)).to(self.device)
+        z[1:1 + 2 * p2] = random_fr(2 * p2, wseed, SID_WIT, device=self.device)
+        a, b, c = (m.desc() for m in self.mats)
+        s = stream_ptr(None)
+        for r0, r1 in ((0, p3), (p3, p3 + p2)):
+            _capi.call("lzk_r1cs_solve", ctypes.byref(a), ctypes.byref(b), ctypes.byref(c), ptr(z), r0, r1, s)
+        return z
+
+    unsatisfied_rows = Circuit.unsatisfied_rows
+
