@@ -270,6 +270,19 @@ size_t lzk_prover_device_bytes(const lzk_prover* prover);
 int lzk_groth16_prove(lzk_prover* prover, const lzk_fr_t* z, const lzk_fr_t* r, const lzk_fr_t* s,
                       lzk_groth16_proof* proof, void* stream);
 
+/* Proof wire format (LZK_PROOF_WIRE_BYTES): the affine coordinates of A, B
+ * and C as canonical (not Montgomery) little-endian 256-bit integers, in the
+ * order A.x, A.y, B.x.c0, B.x.c1, B.y.c0, B.y.c1, C.x, C.y; a point at
+ * infinity is all zeros.  These are the numbers Groth16::Prove prints as its
+ * proof (groth16.cuh:219-221, via print() of the affine point).  Both calls
+ * take device memory and are enqueued on `stream`.  from_wire writes
+ * Jacobian points with Z = 1 (infinity as (0, 1, 0)); a coordinate >= p sets
+ * *bad (device uint32, may be NULL) to 1 and decodes that point as
+ * infinity. */
+#define LZK_PROOF_WIRE_BYTES 256
+int lzk_groth16_proof_to_wire(const lzk_groth16_proof* proof, void* wire, void* stream);
+int lzk_groth16_proof_from_wire(const void* wire, lzk_groth16_proof* proof, uint32_t* bad, void* stream);
+
 /* -------------------------------------------------------------- serving
  * A prove-request server over resident provers with continuous batching.
  * A worker thread admits queued requests (oldest first) into proof

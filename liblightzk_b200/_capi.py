@@ -45,6 +45,8 @@ SIGNATURES = {
     "lzk_prover_destroy": (c_i, [c_p]),
     "lzk_prover_device_bytes": (c_sz, [c_p]),
     "lzk_groth16_prove": (c_i, [c_p, c_p, c_p, c_p, c_p, c_p]),
+    "lzk_groth16_proof_to_wire": (c_i, [c_p, c_p, c_p]),
+    "lzk_groth16_proof_from_wire": (c_i, [c_p, c_p, c_p, c_p]),
     "lzk_server_create": (c_i, [c_p, c_p]),
     "lzk_server_add_circuit": (c_i, [c_p, c_p, c_p]),
     "lzk_server_submit": (c_i, [c_p, c_u32, c_p, c_p, c_p, c_u32, c_p]),

@@ -393,11 +393,88 @@ int prove_ctx(const lzk_prover* p, ProveCtx* x, const Fr* z, const lzk_fr_t* r, 
     return launch_status();
 }
 
+// ---------------- proof wire format ----------------
+// Affine coordinates as canonical little-endian integers; infinity = zeros.
+__device__ __forceinline__ Fq wire_out(const Fq& a) { return from_mont(a); }
+__device__ __forceinline__ Fq2 wire_out(const Fq2& a) { return {from_mont(a.c0), from_mont(a.c1)}; }
+__device__ __forceinline__ Fq wire_in(const Fq& a) { return to_mont(a); }
+__device__ __forceinline__ Fq2 wire_in(const Fq2& a) { return {to_mont(a.c0), to_mont(a.c1)}; }
+
+// a < p, compared limb by limb from the top
+__device__ __forceinline__ bool canonical(const Fq& a)
+{
+    for (int i = 7; i >= 0; i--) {
+        if (a.v[i] != FqP::p(i)) return a.v[i] < FqP::p(i);
+    }
+    return false;
+}
+__device__ __forceinline__ bool canonical(const Fq2& a) { return canonical(a.c0) && canonical(a.c1); }
+
+template <class F>
+__device__ void point_to_wire(const Jac<F>& J, Aff<F>* w)
+{
+    if (J.Z.is_zero()) { *w = Aff<F>{F::zero(), F::zero()}; return; }
+    F zi = inverse(J.Z);
+    F zi2 = mul(zi, zi);
+    *w = Aff<F>{wire_out(mul(J.X, zi2)), wire_out(mul(J.Y, mul(zi2, zi)))};
+}
+
+template <class F>
+__device__ void point_from_wire(const Aff<F>& w, Jac<F>* J, uint32_t* bad)
+{
+    if (w.x.is_zero() && w.y.is_zero()) { *J = Jac<F>{F::zero(), F::one(), F::zero()}; return; }
+    if (!canonical(w.x) || !canonical(w.y)) {
+        if (bad) *bad = 1u;
+        *J = Jac<F>{F::zero(), F::one(), F::zero()};
+        return;
+    }
+    *J = Jac<F>{wire_in(w.x), wire_in(w.y), F::one()};
+}
+
+// one thread per proof point: 0 = A, 1 = B, 2 = C
+__global__ void k_proof_to_wire(const Jac<Fq>* A, const Jac<Fq2>* B, const Jac<Fq>* C, uint32_t* wire)
+{
+    Aff<Fq>* w1 = reinterpret_cast<Aff<Fq>*>(wire);
+    if (threadIdx.x == 0) point_to_wire(*A, w1);
+    if (threadIdx.x == 1) point_to_wire(*B, reinterpret_cast<Aff<Fq2>*>(wire + 16));
+    if (threadIdx.x == 2) point_to_wire(*C, reinterpret_cast<Aff<Fq>*>(wire + 48));
+}
+
+__global__ void k_proof_from_wire(const uint32_t* wire, Jac<Fq>* A, Jac<Fq2>* B, Jac<Fq>* C, uint32_t* bad)
+{
+    if (threadIdx.x == 0) point_from_wire(*reinterpret_cast<const Aff<Fq>*>(wire), A, bad);
+    if (threadIdx.x == 1) point_from_wire(*reinterpret_cast<const Aff<Fq2>*>(wire + 16), B, bad);
+    if (threadIdx.x == 2) point_from_wire(*reinterpret_cast<const Aff<Fq>*>(wire + 48), C, bad);
+}
+
 }  // namespace lzk
 
 using namespace lzk;
 
 extern "C" {
+
+int lzk_groth16_proof_to_wire(const lzk_groth16_proof* proof, void* wire, void* stream)
+{
+    if (!proof || !wire) return LZK_EINVAL;
+    if (reinterpret_cast<uintptr_t>(proof) % 4 || reinterpret_cast<uintptr_t>(wire) % 4) return LZK_EINVAL;
+    k_proof_to_wire<<<1, 32, 0, as_stream(stream)>>>(reinterpret_cast<const Jac<Fq>*>(&proof->A),
+                                                     reinterpret_cast<const Jac<Fq2>*>(&proof->B),
+                                                     reinterpret_cast<const Jac<Fq>*>(&proof->C),
+                                                     static_cast<uint32_t*>(wire)); note_launch();
+    return launch_status();
+}
+
+int lzk_groth16_proof_from_wire(const void* wire, lzk_groth16_proof* proof, uint32_t* bad, void* stream)
+{
+    if (!proof || !wire) return LZK_EINVAL;
+    if (reinterpret_cast<uintptr_t>(proof) % 4 || reinterpret_cast<uintptr_t>(wire) % 4) return LZK_EINVAL;
+    if (bad) LZK_CUDA(cudaMemsetAsync(bad, 0, sizeof(uint32_t), as_stream(stream)));
+    k_proof_from_wire<<<1, 32, 0, as_stream(stream)>>>(static_cast<const uint32_t*>(wire),
+                                                       reinterpret_cast<Jac<Fq>*>(&proof->A),
+                                                       reinterpret_cast<Jac<Fq2>*>(&proof->B),
+                                                       reinterpret_cast<Jac<Fq>*>(&proof->C), bad); note_launch();
+    return launch_status();
+}
 
 int lzk_prover_create(const lzk_groth16_circuit* c, const lzk_groth16_pk* pk, int mode, uint32_t window_bits,
                       lzk_prover** out)

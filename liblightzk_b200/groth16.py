@@ -66,6 +66,26 @@ def split_proof(proof):
     return p[:12].reshape(3, 4), p[12:36].reshape(3, 2, 4), p[36:48].reshape(3, 4)
 
 
+WIRE_BYTES = 256
+
+
+def to_wire(proof, stream=None):
+    """device proof (48 int64 words) -> its 256-byte wire form (device, 32
+    int64 words): affine A, B, C as canonical little-endian integers"""
+    wire = torch.empty(WIRE_BYTES // 8, dtype=torch.int64, device=proof.device)
+    _capi.call("lzk_groth16_proof_to_wire", ptr(proof), ptr(wire), stream_ptr(stream))
+    return wire
+
+
+def from_wire(wire, stream=None):
+    """wire form (device) -> (proof with Z = 1, flag tensor: 1 if a
+    coordinate was not canonical)"""
+    proof = torch.empty(PROOF_WORDS, dtype=torch.int64, device=wire.device)
+    bad = torch.zeros(1, dtype=torch.int32, device=wire.device)
+    _capi.call("lzk_groth16_proof_from_wire", ptr(wire), ptr(proof), ptr(bad), stream_ptr(stream))
+    return proof, bad
+
+
 class Prover:
     def __init__(self, circuit, pk, mode=STANDARD, window_bits=0):
         self.circuit = circuit   # keeps the CSR tensors alive

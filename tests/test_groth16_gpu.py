@@ -102,3 +102,46 @@ def test_modes_differ_only_in_h(cuda, orc, rng_state):
     p1 = groth16.split_proof(groth16.Prover(circ, pk, mode=1, window_bits=8).prove(z, r, s))
     assert same_point(orc, 1, p0[0], p1[0]) and same_point(orc, 2, p0[1], p1[1])
     assert not same_point(orc, 1, p0[2], p1[2])
+
+
+def test_proof_wire_format(cuda, orc, rng_state):
+    """the 256-byte wire form is the affine proof in canonical integers (the
+    numbers Groth16::Prove prints, groth16.cuh:219-221); decoding gives the
+    same points; infinity is all zeros; a coordinate >= p is flagged"""
+    from oracle import FQ
+
+    from liblightzk_b200 import groth16
+    circ, z, pk = _instance(5)
+    r, s = orc.rand_field(FR, 2, rng_state)
+    prover = groth16.Prover(circ, pk, mode=0, window_bits=8)
+    proof = prover.prove(z, r, s)
+    A, B, C = groth16.split_proof(proof)
+    wire = _host(groth16.to_wire(proof)).reshape(8, 4)
+    expect = np.concatenate([orc.from_mont(FQ, orc.jac_to_aff(1, A[None])[0]),
+                             orc.from_mont(FQ, orc.jac_to_aff(2, B[None])[0].reshape(4, 4)),
+                             orc.from_mont(FQ, orc.jac_to_aff(1, C[None])[0])])
+    assert (wire == expect).all()
+    back, bad = groth16.from_wire(groth16.to_wire(proof))
+    assert int(bad.item()) == 0
+    A2, B2, C2 = groth16.split_proof(back)
+    assert same_point(orc, 1, A, A2) and same_point(orc, 2, B, B2) and same_point(orc, 1, C, C2)
+    # A at infinity (libff's (0, 1, 0)) encodes as zeros and decodes back
+    one = orc.to_mont(FQ, np.array([[1, 0, 0, 0]], np.uint64))[0]
+    pinf = proof.clone()
+    pinf[0:12] = torch_tensor(np.concatenate([np.zeros(4, np.uint64), one, np.zeros(4, np.uint64)]), proof.device)
+    w = groth16.to_wire(pinf)
+    assert (_host(w).reshape(8, 4)[0:2] == 0).all()
+    back, bad = groth16.from_wire(w)
+    assert int(bad.item()) == 0 and (_host(back)[0:12].reshape(3, 4)[2] == 0).all()
+    # a coordinate equal to p is not canonical: flagged, decoded as infinity
+    p_limbs = np.array([0x3C208C16D87CFD47, 0x97816A916871CA8D, 0xB85045B68181585D, 0x30644E72E131A029], np.uint64)
+    wb = _host(groth16.to_wire(proof)).copy()
+    wb[0:4] = p_limbs
+    back, bad = groth16.from_wire(torch_tensor(wb, proof.device))
+    assert int(bad.item()) == 1 and (_host(back)[0:12].reshape(3, 4)[2] == 0).all()
+    prover.close()
+
+
+def torch_tensor(a, dev):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a, np.uint64).view(np.int64)).to(dev)
