@@ -54,6 +54,7 @@ def parse():
                          "reference-gpu times the reference's own GPU programs (built by make -C oracle refgpu)")
     ap.add_argument("--log-n", type=int, default=20)
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--plain", action="store_true", help="msm cases: plain affine bases instead of a shifted table")
     ap.add_argument("--inflight", type=int, default=4)
     ap.add_argument("--requests", type=int, default=48)
     return ap.parse_args()
@@ -395,11 +396,14 @@ def run_case(args):
     if args.case in ("msm-g1", "msm-g2"):
         g = 1 if args.case == "msm-g1" else 2
         bases = synth.fixed_base(g, synth.random_fr(n, 5, 78))
-        c = args.window
-        W = msm.windows_for(c)
-        table = msm.precompute(g, bases, c, W, n)
-        ws = torch.empty(msm.workspace_bytes(g, n, c, True, n), dtype=torch.uint8, device="cuda")
-        fn = lambda: msm.msm_precomputed(g, sc, table, c, W, n, workspace=ws)  # noqa: E731
+        if args.plain:
+            fn = lambda: msm.msm(g, sc, bases)  # noqa: E731   (autotuned window)
+        else:
+            c = args.window
+            W = msm.windows_for(c)
+            table = msm.precompute(g, bases, c, W, n)
+            ws = torch.empty(msm.workspace_bytes(g, n, c, True, n), dtype=torch.uint8, device="cuda")
+            fn = lambda: msm.msm_precomputed(g, sc, table, c, W, n, workspace=ws)  # noqa: E731
     else:
         ntt.prepare(args.log_n)
         fn = lambda: ntt.ntt(sc, args.log_n, ntt.COSET_FORWARD)  # noqa: E731
@@ -418,7 +422,7 @@ def run_case(args):
         if last:
             _capi.trace_enable(False)
             if args.case in ("msm-g1", "msm-g2"):
-                for st in ("sort", "accumulate", "fixup", "reduce"):
+                for st in ("sort", "accumulate", "fixup", "reduce", "finish"):
                     stages[st] = _capi.trace_get(f"msm_g{g}_{st}")[0]
     print(json.dumps({"case": args.case, "log_n": args.log_n, "window": args.window, "ms": out,
                       "stages_ms": stages}), flush=True)
@@ -530,6 +534,7 @@ def main():
     # ---------------- G1 MSM at 2^20 (precomputed table, as msm-check.cu) ----------------
     g1_ms = g1_plain_ms = None
     iso_ms = iso_n = iso_pts = 0
+    other = {}
     if rank == 0:
         n = 1 << 20
         sc = synth.random_fr(n, 5, 77, device=dev)
@@ -565,6 +570,33 @@ def main():
             if it >= 2:
                 times.append(a.elapsed_time(b))
         g1_plain_ms = float(np.median(times))
+
+        # ---------------- the other configurations of the benchmark set ----------------
+        def timed(fn, reps=5, warm=3):
+            out = []
+            for it in range(warm + reps):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record()
+                fn()
+                b.record()
+                torch.cuda.synchronize()
+                if it >= warm:
+                    out.append(a.elapsed_time(b))
+            return float(np.median(out))
+        from liblightzk_b200 import ntt
+        n16 = 1 << 16
+        s16, b16 = sc[:n16], bases[:n16]
+        other["g1_msm_2e16_plain_ms"] = timed(lambda: msm.msm(1, s16, b16))
+        if pk.b2.shape[0] >= n:
+            t2 = msm.precompute(2, pk.b2[:n], c, W, n)
+            ws2 = torch.empty(msm.workspace_bytes(2, n, c, True, n), dtype=torch.uint8, device=dev)
+            other["g2_msm_2e20_ms"] = timed(lambda: msm.msm_precomputed(2, sc, t2, c, W, n, workspace=ws2))
+            del t2, ws2
+        big = synth.random_fr(1 << 24, 6, 80, device=dev)
+        ntt.prepare(24)
+        other["ntt_coset_fwd_2e24_ms"] = timed(lambda: ntt.ntt(big, 24, ntt.COSET_FORWARD), reps=3, warm=1)
+        other["ntt_coset_inv_2e24_ms"] = timed(lambda: ntt.ntt(big, 24, ntt.COSET_INVERSE), reps=3, warm=1)
+        del big
 
     if dist:
         dist.barrier()
@@ -611,6 +643,7 @@ def main():
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                        "mean": float(np.mean(lat))},
         "g1_msm_2e20_ms": g1_ms, "g1_msm_2e20_plain_ms": g1_plain_ms,
+        "other_configs_ms": other,
         "e2e": {"value": world * args.steps / (e2e_ms * 1e-3), "unit": "proofs/s",
                 "h2d_bytes_per_step": int(wits[0].numel() * 8), "d2h_bytes_per_step": groth16.PROOF_WORDS * 8},
         "gpu_launches": launches,

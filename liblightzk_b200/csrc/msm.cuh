@@ -404,7 +404,9 @@ int run_msm(const Fr* scalars, const void* bases, size_t n, Jac<typename Gp::F>*
         pp ^= 1;
         if (m == 1) break;
     }
+    void* tr_fin = trace_begin(sizeof(F) == 32 ? "msm_g1_finish" : "msm_g2_finish", st);
     k_finish<F><<<1, 32, 0, st>>>(resA, p.wb, c, out); note_launch();
+    trace_end(tr_fin, st);
     trace_end(tr_red, st);
     trace_end(tr_all, st);
     return launch_status();
