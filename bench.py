@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--matmul-p", type=int, default=100)
     ap.add_argument("--window", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", choices=["prove", "msm-g1", "msm-g2", "ntt", "batch", "serve", "reference-gpu"],
+    ap.add_argument("--case", choices=["prove", "msm-g1", "msm-g2", "ntt", "spmv", "batch", "serve", "reference-gpu"],
                     default="prove",
                     help="prove = the benchmark; msm-g1/msm-g2/ntt run one operator at --log-n for profiling; "
                          "reference-gpu times the reference's own GPU programs (built by make -C oracle refgpu)")
@@ -203,6 +203,33 @@ def run_reference_arm(args, rank, world):
 
 
 # --------------------------------------------------------------- GPU side
+def hbm_peak_gbs():
+    """the measured copy bandwidth of this pool's B200s (MEASURED_PEAKS.json),
+    else the profiling recipe's fallback"""
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def spmv_bytes(circ):
+    """algorithmic bytes of A.z, B.z, C.z: per matrix nnz (32 B value +
+    index + 32 B z gather) + rows (row offset + 32 B output)"""
+    tot = 0
+    for m in circ.mats:
+        ib = m.col.element_size()
+        tot += m.nnz * (32 + ib + 32) + m.rows * (ib + 32)
+    return tot
+
+
+def ntt_algorithmic(log_n, coset=True):
+    """IMAD-class operations and bytes of one transform of 2^log_n: (n/2) log n
+    butterfly products (+ n for the coset scaling) at 264 each; two passes
+    reading and writing 32 B per element"""
+    n = 1 << log_n
+    return ((n // 2) * log_n + (n if coset else 0)) * IMAD_PER_FP_MUL, 2 * 2 * 32 * n
+
+
 def run_reference_gpu_case(args):
     """The reference's own GPU path on this GPU, as its test programs run it:
     oracle/_ref/groth16_gpu is test/groth16.cu (Groth16_BN254 with
@@ -390,6 +417,21 @@ def run_case(args):
         return run_serve_case(args)
     if args.case == "reference-gpu":
         return run_reference_gpu_case(args)
+    if args.case == "spmv":
+        circ = synth.Circuit(args.log_n, seed=1)
+        z = circ.witness(5)
+        outs = [torch.zeros((circ.M, 4), dtype=torch.int64, device="cuda") for _ in range(3)]
+        fn = lambda: ntt.spmv3(circ.A.desc(), circ.B.desc(), circ.C.desc(), z, *outs)  # noqa: E731
+        times = []
+        for _ in range(args.reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            times.append(a.elapsed_time(b))
+        print(json.dumps({"case": "spmv", "log_n": args.log_n, "ms": times, "bytes": spmv_bytes(circ)}), flush=True)
+        return
     n = 1 << args.log_n
     sc = synth.random_fr(n, 5, 77)
     out = []
@@ -597,6 +639,9 @@ def main():
         other["ntt_coset_fwd_2e24_ms"] = timed(lambda: ntt.ntt(big, 24, ntt.COSET_FORWARD), reps=3, warm=1)
         other["ntt_coset_inv_2e24_ms"] = timed(lambda: ntt.ntt(big, 24, ntt.COSET_INVERSE), reps=3, warm=1)
         del big
+        outs = [torch.zeros((circ.M, 4), dtype=torch.int64, device=dev) for _ in range(3)]
+        other["spmv3_ms"] = timed(lambda: ntt.spmv3(circ.A.desc(), circ.B.desc(), circ.C.desc(), wits[0], *outs))
+        del outs
 
     if dist:
         dist.barrier()
@@ -631,6 +676,24 @@ def main():
                     "frac": iso_alg / (iso_avg * 1e-3) / imad_peak,
                     "traffic_bytes": traffic * iso_pts / (avg_pts if avg_pts else 1) if traffic else None}
 
+    rooflines_other = {}
+    hbm, hbm_src = hbm_peak_gbs()
+    if "ntt_coset_fwd_2e24_ms" in other:
+        imad, nbytes = ntt_algorithmic(24)
+        t = other["ntt_coset_fwd_2e24_ms"] * 1e-3
+        rooflines_other["ntt_coset_fwd_2e24"] = {
+            "ms": other["ntt_coset_fwd_2e24_ms"], "imad_achieved_T": imad / t / 1e12,
+            "imad_frac": imad / t / imad_peak, "hbm_gbs": nbytes / t / 1e9, "hbm_frac": nbytes / t / 1e9 / hbm,
+            "bound": "int"}
+    if "spmv3_ms" in other:
+        nbytes = spmv_bytes(circ)
+        t = other["spmv3_ms"] * 1e-3
+        rooflines_other["spmv3_2e20"] = {"ms": other["spmv3_ms"], "bytes": nbytes, "hbm_gbs": nbytes / t / 1e9,
+                                         "hbm_frac": nbytes / t / 1e9 / hbm, "bound": "hbm"}
+    if rooflines_other:
+        rooflines_other["hbm_peak_gbs"] = hbm
+        rooflines_other["hbm_peak_source"] = hbm_src
+
     proofs_s = world * args.steps / (ms_total * 1e-3)
     line = {
         "metric": METRIC, "value": proofs_s, "unit": "proofs/s", "n_gpus": world, "steps": args.steps,
@@ -644,6 +707,7 @@ def main():
                        "mean": float(np.mean(lat))},
         "g1_msm_2e20_ms": g1_ms, "g1_msm_2e20_plain_ms": g1_plain_ms,
         "other_configs_ms": other,
+        "rooflines_other": rooflines_other,
         "e2e": {"value": world * args.steps / (e2e_ms * 1e-3), "unit": "proofs/s",
                 "h2d_bytes_per_step": int(wits[0].numel() * 8), "d2h_bytes_per_step": groth16.PROOF_WORDS * 8},
         "gpu_launches": launches,
