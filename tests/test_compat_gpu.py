@@ -121,3 +121,37 @@ def test_reference_layout_plain_bases(cuda, orc, rng_state, g):
     cfg.base_layout = 2 if g == 1 else 1   # the other group's layout is refused
     st = getattr(_capi.lib(), f"lzk_msm_g{g}")(ds.data_ptr(), dr.data_ptr(), n, out.data_ptr(), ctypes.byref(cfg), None)
     assert st == -1
+
+
+def test_groth16_class(cuda, orc, tmp_path):
+    """Groth16_BN254(input_scale::MatMul_p_39).Setup(12).Prove() from a C++
+    program (tests/compat/groth16_check.cpp, the shape of test/groth16.cu)
+    gives the proof the Python prover gives on the same seeded instance,
+    in the reference's chain mode; its printed affine coordinates are the
+    wire form's numbers."""
+    from liblightzk_b200 import device, groth16, synth
+    libdir = os.path.join(ROOT, "liblightzk_b200")
+    exe = os.path.join(str(tmp_path), "groth16_check")
+    cmd = ["/usr/bin/g++", "-std=c++17", "-O1", "-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include",
+           os.path.join(ROOT, "tests", "compat", "groth16_check.cpp"), "-o", exe, "-L", libdir, "-llzk_b200",
+           "-L", "/usr/local/cuda/lib64", "-lcudart", f"-Wl,-rpath,{libdir}"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    seed = 7
+    r = subprocess.run([exe, str(seed)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    lines = r.stdout.splitlines()
+    wire = np.array([int(x, 16) for x in next(l for l in lines if l.startswith("WIRE")).split()[1:]], np.uint32)
+    # the printed proof: A (x, y), C (x, y), B (x.c0, x.c1, y.c0, y.c1), most significant digit first
+    hexes = [l for l in lines if len(l) == 64]
+    order = [0, 1, 6, 7, 2, 3, 4, 5]          # wire coordinates in print order
+    assert [int(h, 16) for h in hexes] == [int("".join(f"{w:08x}" for w in wire[8 * k:8 * k + 8][::-1]), 16)
+                                           for k in order]
+    circ = synth.MatMulCircuit(39)
+    z = circ.witness(seed + 100)
+    pk = synth.ProvingKey(circ, seed=seed)
+    rs = device.to_host(synth.random_fr(2, seed + 200, 99))
+    prover = groth16.Prover(circ, pk, mode=groth16.REFERENCE, window_bits=12)
+    want = device.to_host(groth16.to_wire(prover.prove(z, rs[0], rs[1]))).view(np.uint32)
+    prover.close()
+    assert (wire == want).all()

@@ -26,3 +26,10 @@ def test_compat_driver_compiles(tmp_path):
         pytest.skip("CUDA headers not installed")
     _cc(["/usr/bin/g++", "-std=c++17", "-Wall", "-fsyntax-only", "-I", INC, "-I", CUDA_INC,
          os.path.join(ROOT, "tests", "compat", "msm_check.cpp")])
+
+
+def test_groth16_class_compiles(tmp_path):
+    if not os.path.isdir(CUDA_INC):
+        pytest.skip("CUDA headers not installed")
+    _cc(["/usr/bin/g++", "-std=c++17", "-Wall", "-fsyntax-only", "-I", INC, "-I", CUDA_INC,
+         os.path.join(ROOT, "tests", "compat", "groth16_check.cpp")])
