@@ -729,6 +729,8 @@ def main():
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_reference_sample(log_m, circ.n_vars, nl)
     print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
 
 
 if __name__ == "__main__":
