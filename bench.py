@@ -552,18 +552,38 @@ def main():
     clk = clocks.stop()
 
     # ---------------- timed: end to end through host memory ----------------
-    zdev = torch.empty_like(wits[0])
+    # Each step copies its witness from pinned host memory and reads its proof
+    # back; the witness of step k + 1 is copied on a second stream into the
+    # other of two device buffers while proof k runs (double buffering, as a
+    # serving loop would), and every copy lies inside the timed region.
+    zbuf = [torch.empty_like(wits[0]) for _ in range(2)]
     host_proofs = torch.empty((args.steps, groth16.PROOF_WORDS), dtype=torch.int64).pin_memory()
+    main = torch.cuda.current_stream()
+    cs = torch.cuda.Stream()
+    ev_in = [torch.cuda.Event() for _ in range(2)]
+    ev_free = [torch.cuda.Event() for _ in range(2)]
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    f0.record()
+    f0.record(main)
+    cs.wait_event(f0)
+    with torch.cuda.stream(cs):
+        zbuf[0].copy_(pinned[0], non_blocking=True)
+        ev_in[0].record(cs)
     for k in range(args.steps):
-        zdev.copy_(pinned[k % nw], non_blocking=True)
-        p = prover.prove(zdev, rs[args.warmup + k, 0], rs[args.warmup + k, 1], proof=proofs[args.warmup + k])
+        cur, nxt = k & 1, (k + 1) & 1
+        if k + 1 < args.steps:
+            with torch.cuda.stream(cs):
+                if k >= 1:
+                    cs.wait_event(ev_free[nxt])      # proof k - 1 has finished with that buffer
+                zbuf[nxt].copy_(pinned[(k + 1) % nw], non_blocking=True)
+                ev_in[nxt].record(cs)
+        main.wait_event(ev_in[cur])
+        p = prover.prove(zbuf[cur], rs[args.warmup + k, 0], rs[args.warmup + k, 1], proof=proofs[args.warmup + k])
+        ev_free[cur].record(main)
         host_proofs[k].copy_(p, non_blocking=True)
-    f1.record()
+    f1.record(main)
     torch.cuda.synchronize()
     e2e_ms = f0.elapsed_time(f1)
 
