@@ -46,7 +46,7 @@ def parse():
                     help="synthetic = the benchmark circuit (--log-m); matmul = the reference's own MatMul "
                          "circuit (--matmul-p; p = 100 gives 2^20 constraints)")
     ap.add_argument("--matmul-p", type=int, default=100)
-    ap.add_argument("--window", type=int, default=16)
+    ap.add_argument("--window", type=int, default=17)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--case", choices=["prove", "msm-g1", "msm-g2", "ntt", "spmv", "batch", "serve", "reference-gpu"],
                     default="prove",

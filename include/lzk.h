@@ -258,7 +258,7 @@ typedef struct lzk_groth16_proof {
 
 typedef struct lzk_prover lzk_prover;
 
-/* window_bits: MSM window of the resident tables (0 = 16).  The query
+/* window_bits: MSM window of the resident tables (0 = 17).  The query
  * arrays of pk are read only during creation; the circuit's CSR arrays must
  * stay valid while the prover lives. */
 int lzk_prover_create(const lzk_groth16_circuit* circuit, const lzk_groth16_pk* pk, int mode,

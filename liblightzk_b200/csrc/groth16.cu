@@ -247,7 +247,7 @@ static int create(const lzk_groth16_circuit* c, const lzk_groth16_pk* pk, int mo
     p->n_public = c->n_public;
     if (!pk->a_query || !pk->b1_query || !pk->b2_query || !pk->h_query || (!pk->l_query && c->n_vars > c->n_public + 1))
         return LZK_EINVAL;
-    p->c = window_bits ? window_bits : 16;
+    p->c = window_bits ? window_bits : 17;
     if (p->c < 2 || p->c > 24) return LZK_EINVAL;
     p->wins = windows_for(p->c);
 
