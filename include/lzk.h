@@ -381,6 +381,17 @@ void lzk_trace_reset(void);
 /* Total device milliseconds and count of completed regions named `name`
  * since the last reset (waits for pending regions). */
 int lzk_trace_get(const char* name, double* total_ms, uint64_t* count);
+/* The completed regions since the last reset as a timeline: device
+ * milliseconds from the start of the first region begun after the reset,
+ * in completion-resolution order (at most 65 536 kept).  Writes up to `cap`
+ * spans and sets *count to the number held.  Shows which stream's work ends
+ * a multi-stream call such as a proof. */
+typedef struct lzk_trace_span {
+    char name[40];
+    double start_ms;
+    double end_ms;
+} lzk_trace_span;
+int lzk_trace_timeline(lzk_trace_span* spans, size_t cap, size_t* count);
 /* Number of kernels this library has launched so far (all devices). */
 uint64_t lzk_launch_count(void);
 /* Measured 32-bit integer multiply-add rate of the current device

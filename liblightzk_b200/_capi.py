@@ -64,6 +64,7 @@ SIGNATURES = {
     "lzk_trace_enable": (None, [c_i]),
     "lzk_trace_reset": (None, []),
     "lzk_trace_get": (c_i, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64)]),
+    "lzk_trace_timeline": (c_i, [c_p, c_sz, ctypes.POINTER(c_sz)]),
     "lzk_probe_imad_rate": (c_i, [ctypes.POINTER(ctypes.c_double)]),
     "lzk_launch_count": (ctypes.c_uint64, []),
 }
@@ -165,6 +166,20 @@ def trace_get(name):
     ms, cnt = ctypes.c_double(), ctypes.c_uint64()
     call("lzk_trace_get", name.encode(), ctypes.byref(ms), ctypes.byref(cnt))
     return ms.value, cnt.value
+
+
+class TraceSpan(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 40), ("start_ms", ctypes.c_double), ("end_ms", ctypes.c_double)]
+
+
+def trace_timeline():
+    """[(name, start ms, end ms)] of the regions completed since the last
+    reset, on one device clock whose zero is the first region's start"""
+    n = ctypes.c_size_t()
+    call("lzk_trace_timeline", None, 0, ctypes.byref(n))
+    buf = (TraceSpan * max(n.value, 1))()
+    call("lzk_trace_timeline", buf, n.value, ctypes.byref(n))
+    return [(t.name.decode(), t.start_ms, t.end_ms) for t in buf[:n.value]]
 
 
 def probe_imad_rate():

@@ -152,29 +152,13 @@ static int run_plan(lzk_batch_plan* p, cudaStream_t st)
         constexpr unsigned fx_threads = 32768 / sizeof(X);
         k_fixup_large<F><<<148 * 2, fx_threads, fx_threads * sizeof(X), st>>>(p->off, bsum, static_cast<X*>(p->head),
                                                                              static_cast<X*>(p->tail), p->large); note_launch();
-        // one reduction chain per window width
+        // one bucket reduction per window width
         uint64_t wdone = 0;
         for (auto& wg : p->wgroups) {
-            const X* inR = bsum + wg.bucket_base;
-            const X* inA = nullptr;
-            const uint32_t* offp = p->off + wg.bucket_base;
-            uint32_t m = 1u << (wg.c - 1), logM = 0, base1 = 1, pp = 0;
-            while (true) {
-                uint32_t L = m < kLevelL ? m : kLevelL;
-                uint32_t segs = m / L;
-                bool last = segs == 1;
-                X* outR = static_cast<X*>(p->lr[pp]);
-                X* outA = last ? static_cast<X*>(p->wres) + wdone : static_cast<X*>(p->la[pp]);
-                size_t threads = (size_t)wg.windows * segs * 32;
-                k_level<F><<<grid_for(threads, 128), 128, 0, st>>>(inR, inA, offp, (uint32_t)wg.windows, m, L, base1, logM,
-                                                                  outR, outA); note_launch();
-                inR = outR; inA = outA; offp = nullptr; base1 = 0;
-                uint32_t lg = 0; while ((1u << lg) < L) lg++;
-                logM += lg;
-                m = segs;
-                pp ^= 1;
-                if (last) break;
-            }
+            LZK_TRY(reduce_buckets<F>(bsum + wg.bucket_base, p->off + wg.bucket_base, (uint32_t)wg.windows,
+                                      1u << (wg.c - 1), static_cast<X*>(p->lr[0]), static_cast<X*>(p->la[0]),
+                                      static_cast<X*>(p->lr[1]), static_cast<X*>(p->la[1]),
+                                      static_cast<X*>(p->wres) + wdone, st));
             wdone += wg.windows;
         }
         k_bfinish<F><<<grid_for(count, 32), 32, 0, st>>>(p->d_desc, count, static_cast<const X*>(p->wres)); note_launch();

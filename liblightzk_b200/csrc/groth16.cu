@@ -319,7 +319,9 @@ int prove_ctx(const lzk_prover* p, ProveCtx* x, const Fr* z, const lzk_fr_t* r, 
     LZK_CUDA(cudaStreamWaitEvent(x->s3, x->ev_fork, 0));
 
     // s3: fixed-base products
+    void* tr_fx = trace_begin("groth16_fixed_products", x->s3);
     k_fixed_products<<<1, 32, 0, x->s3>>>(p->comb1, p->comb2, rs, ss, x->sm1, x->sm2); note_launch();
+    trace_end(tr_fx, x->s3);
 
     // s1: one digit sort of z for the A, B1 and B2 MSMs (same scalars, same
     // window width, tables of the same level stride n_vars)
@@ -345,7 +347,9 @@ int prove_ctx(const lzk_prover* p, ProveCtx* x, const Fr* z, const lzk_fr_t* r, 
     LZK_TRY(msm_tab1(p, x, 1, z, p->n_vars, x->g1res + 1, 1, x->s1, true));
     LZK_CUDA(cudaEventRecord(x->ev_b1, x->s1));
     LZK_CUDA(cudaStreamWaitEvent(x->s3, x->ev_b1, 0));
+    void* tr_dep = trace_begin("groth16_dep_products", x->s3);
     k_dep_products<<<1, 32, 0, x->s3>>>(x->g1res, rs, ss, x->sm1); note_launch();
+    trace_end(tr_dep, x->s3);
     LZK_CUDA(cudaEventRecord(x->ev_s3, x->s3));
     size_t nl = p->n_vars - p->n_public - 1;
     LZK_TRY(msm_tab1(p, x, 2, z + p->n_public + 1, nl, x->g1res + 2, 1, x->s1));
@@ -355,6 +359,7 @@ int prove_ctx(const lzk_prover* p, ProveCtx* x, const Fr* z, const lzk_fr_t* r, 
     Fr* x0 = x->x;
     Fr* x1 = x->x + p->L;
     Fr* x2 = x->x + 2 * p->L;
+    void* tr_h = trace_begin("groth16_h_poly", st);
     LZK_CUDA(cudaMemsetAsync(x->x, 0, 3 * p->L * sizeof(Fr), st));
     lzk_csr none{};
     (void)none;
@@ -382,13 +387,16 @@ int prove_ctx(const lzk_prover* p, ProveCtx* x, const Fr* z, const lzk_fr_t* r, 
         LZK_TRY(ntt_run(x0, p->log_m, LZK_NTT_COSET_INVERSE, 1, 0, nullptr, st));
         hs = x0;
     }
+    trace_end(tr_h, st);
     LZK_TRY(msm_tab1(p, x, 3, hs, p->M - 1, x->g1res + 3, 0, st));
 
     // join and assemble
     LZK_CUDA(cudaStreamWaitEvent(st, x->ev_s1, 0));
     LZK_CUDA(cudaStreamWaitEvent(st, x->ev_s2, 0));
     LZK_CUDA(cudaStreamWaitEvent(st, x->ev_s3, 0));
+    void* tr_as = trace_begin("groth16_assemble", st);
     k_assemble<<<1, 32, 0, st>>>(p->g1c, p->g2c, x->g1res, x->g2res, x->sm1, x->sm2, proof); note_launch();
+    trace_end(tr_as, st);
     trace_end(tr, st);
     return launch_status();
 }

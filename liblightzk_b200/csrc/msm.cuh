@@ -10,7 +10,7 @@ struct G1 { using F = Fq; };
 struct G2 { using F = Fq2; };
 
 constexpr uint32_t kAccChunk = 64;   // sorted entries per accumulation thread
-constexpr uint32_t kLevelL = 32;     // buckets per warp in a reduction level
+constexpr uint32_t kLevelL = 32;     // buckets per warp tile of the bucket reduction
 constexpr uint32_t kFixSmall = 64;   // partials a single fix-up thread folds
 
 struct MsmPlan {
@@ -40,8 +40,8 @@ inline void plan_msm(MsmPlan& p, size_t n, uint32_t c, bool shared, size_t strid
     p.B = p.wb * p.nb;
     p.max_entries = n * (size_t)p.W;
     p.chunks = (p.max_entries + kAccChunk - 1) / kAccChunk;
-    // the first reduction level writes wb * max(1, nb / kLevelL) points; later
-    // levels write fewer
+    // bucket reduction scratch: wb * max(1, nb / kLevelL) points per buffer
+    // (reduce_buckets)
     size_t lvl = (size_t)p.wb * (p.nb > kLevelL ? p.nb / kLevelL : 1);
     Carver cv;
     p.o_cnt = cv.take<uint32_t>(p.B);
@@ -248,51 +248,143 @@ __device__ __forceinline__ XYZZ<F> shfl_pt(const XYZZ<F>& x, uint32_t lane)
     return r;
 }
 
-// One level of the weighted bucket sum, one warp per segment of L <= 32
-// consecutive points.  Per window the input holds m points X_k; for the
-// segment s, lane j holds X_{sL+j}, a shuffle scan forms the suffix sums
-// S_j = sum_{k >= j} X_{sL+k}, and
-//   R_s = S_0,
-//   t_s = sum_{j >= 1 - base} S_j = sum_j (j + base) X_{sL+j},
-//   A_s = sum_j Ain_{sL+j} + 2^logM * t_s,
-// so that sum_k (k + base) X_k = sum_s t_s + L * sum_s s R_s: the next level
-// (base 0) reduces the R_s, and the A's carry the weighted partial results
-// (scaled by the product of the earlier segment lengths) to the top.  Empty
-// buckets (off[k] == off[k+1]) read as the point at infinity.
+// ---------------------------- bucket reduction ----------------------------
+// Per bucket set (one per window for plain bases, one for all windows with a
+// shifted-copy table) of m = 2^(c-1) buckets B_0..B_{m-1}, bucket k holding
+// digit k + 1, the weighted sum W = sum_k (k+1) B_k.  With tiles of
+// L = min(m, 32) buckets and P = m / L tiles,
+//   W = sum_u t_u + L sum_u u R_u = T + sum_{i < log P} 2^(i + log L) G_i,
+// where R_u is the sum of tile u, t_u = sum_j (j+1) B_{uL+j} its locally
+// weighted sum, T = sum_u t_u and G_i = sum of the R_u with bit i of u set
+// (bit slices of the tile index).  Four launches:
+//   k_red_tile     one warp per tile: shuffle suffix scan S_j = sum_{j'>=j}
+//                  B_{uL+j'}, R_u = S_0, t_u = sum_j S_j;
+//   k_red_slices   one warp per 32 members of one of the 1 + log P sums T,
+//                  G_0, G_1, ... (xor-shuffle tree);
+//   k_red_scale    one warp per sum: fold its partials, double it
+//                  i + log L times;
+//   k_red_combine  one warp per set: add the scaled sums.
+// For m = 2^16 the longest chain is 10 + 5 + 6 + 15 doublings + 5 dependent
+// point operations (a ladder of segment levels with the weights carried by
+// doublings at every level needs about twice that), and every operation is a
+// latency-staged one (xyzz_add_cold / xyzz_dbl_cold).  Empty buckets
+// (off[k] == off[k+1]) read as the point at infinity.
 template <class F>
-__global__ void __launch_bounds__(128) k_level(const XYZZ<F>* __restrict__ inR, const XYZZ<F>* __restrict__ inA,
-                                               const uint32_t* __restrict__ off, uint32_t windows, uint32_t m,
-                                               uint32_t L, uint32_t base, uint32_t logM, XYZZ<F>* __restrict__ outR,
-                                               XYZZ<F>* __restrict__ outA)
+__global__ void __launch_bounds__(128) k_red_tile(const XYZZ<F>* __restrict__ bsum, const uint32_t* __restrict__ off,
+                                                  uint32_t wb, uint32_t m, uint32_t L, XYZZ<F>* __restrict__ R,
+                                                  XYZZ<F>* __restrict__ T)
 {
     const uint32_t lane = threadIdx.x & 31;
-    const uint32_t segs = m / L;
-    const uint64_t total = (uint64_t)windows * segs;
-    for (uint64_t seg = gtid() >> 5; seg < total; seg += gstride() >> 5) {
-        uint32_t w = (uint32_t)(seg / segs), s = (uint32_t)(seg % segs);
-        size_t first = (size_t)w * m + (size_t)s * L;
-        XYZZ<F> S = xyzz_inf<F>(), A = xyzz_inf<F>();
-        if (lane < L) {
-            size_t k = first + lane;
-            if (!off || off[k] != off[k + 1]) S = ld_elem(inR + k);
-            if (inA) A = ld_elem(inA + k);
-        }
+    const uint64_t total = (uint64_t)wb * (m / L);
+    for (uint64_t tile = gtid() >> 5; tile < total; tile += gstride() >> 5) {
+        size_t k = (size_t)tile * L + lane;   // = w m + u L + lane
+        XYZZ<F> S = xyzz_inf<F>();
+        if (lane < L && off[k] != off[k + 1]) S = ld_elem(bsum + k);
         for (uint32_t d = 1; d < L; d <<= 1) {
             XYZZ<F> o = shfl_down_pt(S, d);
             if (lane + d < L) S = xyzz_add_cold(S, o);
         }
-        XYZZ<F> R = shfl_pt(S, 0);
-        XYZZ<F> t = (lane < L && (lane >= 1 || base)) ? S : xyzz_inf<F>();
-        for (uint32_t d = 16; d > 0; d >>= 1) {
-            t = xyzz_add_cold(t, shfl_xor_pt(t, d));
-            if (inA) A = xyzz_add_cold(A, shfl_xor_pt(A, d));
-        }
+        XYZZ<F> t = S;
+        for (uint32_t d = L >> 1; d > 0; d >>= 1) t = xyzz_add_cold(t, shfl_xor_pt(t, d));
         if (lane == 0) {
-            for (uint32_t d = 0; d < logM; d++) t = xyzz_dbl_cold(t);
-            st_elem(outR + seg, R);
-            st_elem(outA + seg, xyzz_add_cold(A, t));
+            st_elem(R + tile, S);
+            st_elem(T + tile, t);
         }
     }
+}
+
+struct RedShape {
+    uint32_t L, lgL, P, lg;   // tile size, log2 L, tiles per set, log2 P
+    uint32_t cT, cG, NP, NS;  // chunks of T, chunks of each G_i, partials and sums per set
+};
+inline RedShape red_shape(uint32_t m)
+{
+    RedShape s;
+    s.L = m < 32 ? m : 32;
+    s.lgL = 0; while ((1u << s.lgL) < s.L) s.lgL++;
+    s.P = m / s.L;
+    s.lg = 0; while ((1u << s.lg) < s.P) s.lg++;
+    s.cT = (s.P + 31) / 32;
+    s.cG = (s.P / 2 + 31) / 32;
+    s.NP = s.cT + s.lg * s.cG;
+    s.NS = 1 + s.lg;
+    return s;
+}
+
+// member v of slice i: the v-th tile index with bit i set
+__device__ __forceinline__ uint32_t slice_member(uint32_t v, uint32_t i)
+{
+    return ((v >> i) << (i + 1)) | (1u << i) | (v & ((1u << i) - 1));
+}
+
+template <class F>
+__global__ void __launch_bounds__(128) k_red_slices(const XYZZ<F>* __restrict__ R, const XYZZ<F>* __restrict__ T,
+                                                    uint32_t wb, RedShape sh, XYZZ<F>* __restrict__ part)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t total = (uint64_t)wb * sh.NP;
+    for (uint64_t g = gtid() >> 5; g < total; g += gstride() >> 5) {
+        uint32_t w = (uint32_t)(g / sh.NP), q = (uint32_t)(g % sh.NP);
+        const size_t base = (size_t)w * sh.P;
+        XYZZ<F> x = xyzz_inf<F>();
+        if (q < sh.cT) {
+            uint32_t v = q * 32 + lane;
+            if (v < sh.P) x = ld_elem(T + base + v);
+        } else {
+            uint32_t i = (q - sh.cT) / sh.cG, v = ((q - sh.cT) % sh.cG) * 32 + lane;
+            if (v < sh.P / 2) x = ld_elem(R + base + slice_member(v, i));
+        }
+        for (uint32_t d = 16; d > 0; d >>= 1) x = xyzz_add_cold(x, shfl_xor_pt(x, d));
+        if (lane == 0) st_elem(part + g, x);
+    }
+}
+
+template <class F>
+__global__ void __launch_bounds__(128) k_red_scale(const XYZZ<F>* __restrict__ part, uint32_t wb, RedShape sh,
+                                                   XYZZ<F>* __restrict__ scaled)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t total = (uint64_t)wb * sh.NS;
+    for (uint64_t g = gtid() >> 5; g < total; g += gstride() >> 5) {
+        uint32_t w = (uint32_t)(g / sh.NS), s = (uint32_t)(g % sh.NS);
+        uint32_t first = s == 0 ? 0 : sh.cT + (s - 1) * sh.cG, cnt = s == 0 ? sh.cT : sh.cG;
+        const XYZZ<F>* src = part + (size_t)w * sh.NP + first;
+        XYZZ<F> x = xyzz_inf<F>();
+        for (uint32_t c = lane; c < cnt; c += 32) x = xyzz_add_cold(x, ld_elem(src + c));
+        for (uint32_t d = 16; d > 0; d >>= 1) x = xyzz_add_cold(x, shfl_xor_pt(x, d));
+        if (lane == 0) {
+            uint32_t dbls = s == 0 ? 0 : s - 1 + sh.lgL;
+            for (uint32_t d = 0; d < dbls; d++) x = xyzz_dbl_cold(x);
+            st_elem(scaled + g, x);
+        }
+    }
+}
+
+template <class F>
+__global__ void __launch_bounds__(128) k_red_combine(const XYZZ<F>* __restrict__ scaled, uint32_t wb, uint32_t NS,
+                                                     XYZZ<F>* __restrict__ win)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint64_t w = gtid() >> 5; w < wb; w += gstride() >> 5) {
+        XYZZ<F> x = lane < NS ? ld_elem(scaled + w * NS + lane) : xyzz_inf<F>();
+        for (uint32_t d = 16; d > 0; d >>= 1) x = xyzz_add_cold(x, shfl_xor_pt(x, d));
+        if (lane == 0) st_elem(win + w, x);
+    }
+}
+
+// W_w of wb sets of m buckets (bsum / off indexed w m + k) into win[0..wb).
+// Scratch: R, T of wb * max(1, m / 32) points each; part and scaled fit in
+// the same size (NP, NS <= P).  win may alias R.
+template <class F>
+int reduce_buckets(const XYZZ<F>* bsum, const uint32_t* off, uint32_t wb, uint32_t m, XYZZ<F>* R, XYZZ<F>* T,
+                   XYZZ<F>* part, XYZZ<F>* scaled, XYZZ<F>* win, cudaStream_t st)
+{
+    RedShape sh = red_shape(m);
+    k_red_tile<F><<<grid_for((size_t)wb * sh.P * 32, 128), 128, 0, st>>>(bsum, off, wb, m, sh.L, R, T); note_launch();
+    k_red_slices<F><<<grid_for((size_t)wb * sh.NP * 32, 128), 128, 0, st>>>(R, T, wb, sh, part); note_launch();
+    k_red_scale<F><<<grid_for((size_t)wb * sh.NS * 32, 128), 128, 0, st>>>(part, wb, sh, scaled); note_launch();
+    k_red_combine<F><<<grid_for((size_t)wb * 32, 128), 128, 0, st>>>(scaled, wb, sh.NS, win); note_launch();
+    return launch_status();
 }
 
 template <class F>
@@ -390,24 +482,10 @@ int run_msm(const Fr* scalars, const void* bases, size_t n, Jac<typename Gp::F>*
 
     // weighted sums per bucket set
     void* tr_red = trace_begin(sizeof(F) == 32 ? "msm_g1_reduce" : "msm_g2_reduce", st);
-    const X* inR = bsum; const X* inA = nullptr; const uint32_t* offp = off;
-    uint32_t m = p.nb, logM = 0, base1 = 1, pp = 0;
-    X* resA = nullptr;
-    while (true) {
-        uint32_t L = m < kLevelL ? m : kLevelL;
-        uint32_t segs = m / L;
-        size_t threads = (size_t)p.wb * segs * 32;
-        k_level<F><<<grid_for(threads, 128), 128, 0, st>>>(inR, inA, offp, p.wb, m, L, base1, logM, lr[pp], la[pp]); note_launch();
-        inR = lr[pp]; inA = la[pp]; resA = la[pp];
-        offp = nullptr; base1 = 0;
-        uint32_t lg = 0; while ((1u << lg) < L) lg++;
-        logM += lg;
-        m = segs;
-        pp ^= 1;
-        if (m == 1) break;
-    }
+    X* win = lr[0];
+    LZK_TRY(reduce_buckets<F>(bsum, off, p.wb, p.nb, lr[0], la[0], lr[1], la[1], win, st));
     void* tr_fin = trace_begin(sizeof(F) == 32 ? "msm_g1_finish" : "msm_g2_finish", st);
-    k_finish<F><<<1, 32, 0, st>>>(resA, p.wb, c, out); note_launch();
+    k_finish<F><<<1, 32, 0, st>>>(win, p.wb, c, out); note_launch();
     trace_end(tr_fin, st);
     trace_end(tr_red, st);
     trace_end(tr_all, st);

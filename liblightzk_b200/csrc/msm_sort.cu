@@ -17,9 +17,9 @@
 //                  so a bucket holding most of the entries (all scalars
 //                  equal, or the sparse top window of 254-bit scalars at
 //                  some widths) is summed with logarithmic depth.
-//   6. k_level     weighted bucket sums  sum_j j*B_j  by segmented running
-//                  sums, L buckets per thread, repeated until one value
-//                  per window is left.
+//   6. k_red_*     weighted bucket sums  sum_j j*B_j  per bucket set: warp
+//                  tiles of 32 buckets by shuffle scans, then bit slices of
+//                  the tile index, each doubled to its weight (msm.cuh).
 //   7. k_finish    windows combined by Horner (c doublings per window), or
 //                  nothing to combine when the bases come with precomputed
 //                  2^(c*w) shifts (every window shares one bucket set, the

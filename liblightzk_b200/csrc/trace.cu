@@ -19,10 +19,19 @@ struct TraceRec {
     cudaEvent_t a, b;
 };
 
+struct TraceSpan {
+    std::string name;
+    double start_ms, end_ms;
+};
+
 static std::mutex g_tr_mu;
 static bool g_tr_on = false;
 static std::vector<TraceRec> g_tr_pending;
 static std::map<std::string, std::pair<double, uint64_t>> g_tr_sum;
+// timeline: spans relative to the first region begun since the last reset
+static cudaEvent_t g_tr_origin = nullptr;
+static std::vector<TraceSpan> g_tr_spans;
+constexpr size_t kMaxSpans = 1u << 16;
 
 static std::atomic<unsigned long long> g_launches{0};
 
@@ -36,6 +45,10 @@ void* trace_begin(const char* name, cudaStream_t st)
     TraceRec* r = new TraceRec{name, nullptr, nullptr};
     cudaEventCreate(&r->a);
     cudaEventCreate(&r->b);
+    {
+        std::lock_guard<std::mutex> g(g_tr_mu);
+        if (!g_tr_origin && cudaEventCreate(&g_tr_origin) == cudaSuccess) cudaEventRecord(g_tr_origin, st);
+    }
     cudaEventRecord(r->a, st);
     return r;
 }
@@ -58,6 +71,11 @@ static void resolve()
             auto& s = g_tr_sum[r.name];
             s.first += ms;
             s.second += 1;
+            float t0 = 0.f, t1 = 0.f;
+            if (g_tr_origin && g_tr_spans.size() < kMaxSpans &&
+                cudaEventElapsedTime(&t0, g_tr_origin, r.a) == cudaSuccess &&
+                cudaEventElapsedTime(&t1, g_tr_origin, r.b) == cudaSuccess)
+                g_tr_spans.push_back(TraceSpan{r.name, t0, t1});
         }
         cudaEventDestroy(r.a);
         cudaEventDestroy(r.b);
@@ -104,6 +122,26 @@ void lzk_trace_reset(void)
     std::lock_guard<std::mutex> g(g_tr_mu);
     resolve();
     g_tr_sum.clear();
+    g_tr_spans.clear();
+    if (g_tr_origin) cudaEventDestroy(g_tr_origin);
+    g_tr_origin = nullptr;
+}
+
+int lzk_trace_timeline(lzk_trace_span* spans, size_t cap, size_t* count)
+{
+    if (!count || (cap && !spans)) return LZK_EINVAL;
+    std::lock_guard<std::mutex> g(g_tr_mu);
+    resolve();
+    *count = g_tr_spans.size();
+    for (size_t i = 0; i < cap && i < g_tr_spans.size(); i++) {
+        const TraceSpan& t = g_tr_spans[i];
+        size_t k = 0;
+        for (; k + 1 < sizeof(spans[i].name) && k < t.name.size(); k++) spans[i].name[k] = t.name[k];
+        spans[i].name[k] = 0;
+        spans[i].start_ms = t.start_ms;
+        spans[i].end_ms = t.end_ms;
+    }
+    return LZK_OK;
 }
 
 int lzk_trace_get(const char* name, double* total_ms, uint64_t* count)

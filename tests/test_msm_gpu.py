@@ -32,7 +32,7 @@ def test_g1_config1_2e16(cuda, orc, rng_state):
     assert same_point(orc, 1, _run(1, s, b), orc.msm(1, s, b))
 
 
-@pytest.mark.parametrize("c", [2, 3, 4, 7, 8, 12, 13, 16, 20])
+@pytest.mark.parametrize("c", [2, 3, 4, 5, 6, 7, 8, 12, 13, 16, 17, 20])
 def test_g1_window_widths(cuda, orc, rng_state, c):
     n = 777
     s, b = scalars(orc, n, rng_state), bases(orc, 1, n, rng_state)
@@ -81,7 +81,7 @@ def test_g1_empty(cuda, orc):
     assert orc.jac_to_aff(1, out[None]).sum() == 0
 
 
-@pytest.mark.parametrize("c", [8, 12, 16])
+@pytest.mark.parametrize("c", [8, 12, 16, 17])
 def test_g1_precomputed(cuda, orc, rng_state, c):
     from liblightzk_b200 import device, msm
     n = 3000
@@ -112,6 +112,24 @@ def test_g1_precomputed(cuda, orc, rng_state, c):
 def test_g2_random(cuda, orc, rng_state, n):
     s, b = scalars(orc, n, rng_state), bases(orc, 2, n, rng_state)
     assert same_point(orc, 2, _run(2, s, b), orc.msm(2, s, b))
+
+
+@pytest.mark.parametrize("c", [2, 6, 7, 11])
+def test_g2_window_widths(cuda, orc, rng_state, c):
+    n = 300
+    s, b = scalars(orc, n, rng_state), bases(orc, 2, n, rng_state)
+    assert same_point(orc, 2, _run(2, s, b, c), orc.msm(2, s, b))
+
+
+def test_g2_precomputed_c17(cuda, orc, rng_state):
+    """the prover's width: one bucket set of 2^16 for all 15 windows"""
+    from liblightzk_b200 import device, msm
+    n, c = 2000, 17
+    s, b = scalars(orc, n, rng_state), bases(orc, 2, n, rng_state)
+    W = msm.windows_for(c)
+    table = msm.precompute(2, device.to_device(b), c, W, n)
+    out = device.to_host(msm.msm_precomputed(2, device.to_device(s), table, c, W, n))
+    assert same_point(orc, 2, out, orc.msm(2, s, b))
 
 
 def test_g2_edges_and_precomputed(cuda, orc, rng_state):
