@@ -255,4 +255,96 @@ template <class F> __device__ __forceinline__ XYZZ<F> jac_to_xyzz(const Jac<F>& 
 template <class F> __device__ __noinline__ XYZZ<F> xyzz_add_cold(const XYZZ<F> p, const XYZZ<F> q) { return xyzz_add(p, q); }
 template <class F> __device__ __noinline__ XYZZ<F> xyzz_dbl_cold(const XYZZ<F> p) { return xyzz_dbl(p); }
 
+// ---------------- warp-uniform point operations ----------------
+// For chains of dependent operations on one point (the window combination,
+// the weighting doublings of the bucket reduction, the proof assembly).  A
+// lone warp running such a chain keeps its SM sub-partition's multiplier
+// pipe busy, and a warp instruction costs the same for one active lane as
+// for 32.  So all 32 lanes hold the same operands, each stage of the formula
+// computes its independent products one per lane, and shuffles hand every
+// lane all of them: a stage of up to six products takes the time of one.
+// add-2008-s becomes four dependent stages (6, 2, 3, 3 products) instead of
+// seven pairs, dbl-2008-s-1 three (2, 4, 3) instead of six, with the same
+// products and results as xyzz_add / xyzz_dbl.  Callers: every lane of the
+// warp, converged, with equal arguments; every lane gets the result.
+template <class F>
+__device__ __forceinline__ F shfl_elem(const F& x, int src)
+{
+    F r;
+    const uint32_t* s = reinterpret_cast<const uint32_t*>(&x);
+    uint32_t* o = reinterpret_cast<uint32_t*>(&r);
+    _Pragma("unroll") for (int i = 0; i < (int)(sizeof(F) / 4); i++) o[i] = __shfl_sync(0xffffffffu, s[i], src);
+    return r;
+}
+template <int N, class F>
+__device__ __forceinline__ void warp_products(F (&r)[N], const F (&a)[N], const F (&b)[N])
+{
+    const int lane = threadIdx.x & 31;
+    F x = a[0], y = b[0];
+    _Pragma("unroll") for (int k = 1; k < N; k++) {
+        if (lane == k) { x = a[k]; y = b[k]; }
+    }
+    F z = cmul(x, y);
+    _Pragma("unroll") for (int k = 0; k < N; k++) r[k] = shfl_elem(z, k);
+}
+
+template <class F> __device__ __noinline__ XYZZ<F> xyzz_dbl_warp(const XYZZ<F> p)
+{
+    if (xyzz_is_inf(p)) return p;
+    F U = dbl(p.Y);
+    F s1[2];
+    { F a[2] = {U, p.X}; warp_products<2>(s1, a, a); }
+    F V = s1[0], x2 = s1[1];
+    F M = add(dbl(x2), x2);
+    F s2[4];
+    { F a[4] = {U, p.X, V, M}; F b[4] = {V, V, p.ZZ, M}; warp_products<4>(s2, a, b); }
+    F W = s2[0], S = s2[1], ZZ3 = s2[2], MM = s2[3];
+    F X3 = sub(MM, dbl(S));
+    F s3[3];
+    { F a[3] = {M, W, W}; F b[3] = {sub(S, X3), p.Y, p.ZZZ}; warp_products<3>(s3, a, b); }
+    return {X3, sub(s3[0], s3[1]), ZZ3, s3[2]};
+}
+
+template <class F> __device__ __noinline__ XYZZ<F> xyzz_add_warp(const XYZZ<F> p, const XYZZ<F> q)
+{
+    if (xyzz_is_inf(q)) return p;
+    if (xyzz_is_inf(p)) return q;
+    F s1[6];
+    { F a[6] = {p.X, q.X, p.Y, q.Y, p.ZZ, p.ZZZ}; F b[6] = {q.ZZ, p.ZZ, q.ZZZ, p.ZZZ, q.ZZ, q.ZZZ}; warp_products<6>(s1, a, b); }
+    F U1 = s1[0], S1 = s1[2], zz = s1[4], zzz = s1[5];
+    F P = sub(s1[1], U1);
+    F R = sub(s1[3], S1);
+    if (P.is_zero()) {
+        if (R.is_zero()) return xyzz_dbl_warp(p);
+        return xyzz_inf<F>();
+    }
+    F s2[2];
+    { F a[2] = {P, R}; warp_products<2>(s2, a, a); }
+    F PP = s2[0], RR = s2[1];
+    F s3[3];
+    { F a[3] = {P, U1, zz}; F b[3] = {PP, PP, PP}; warp_products<3>(s3, a, b); }
+    F PPP = s3[0], Q = s3[1], ZZ3 = s3[2];
+    F X3 = sub(sub(RR, PPP), dbl(Q));
+    F s4[3];
+    { F a[3] = {R, S1, zzz}; F b[3] = {sub(Q, X3), PPP, PPP}; warp_products<3>(s4, a, b); }
+    return {X3, sub(s4[0], s4[1]), ZZ3, s4[2]};
+}
+
+// XYZZ -> Jacobian for a whole warp (products in two stages of two and one
+// of two)
+template <class F> __device__ __forceinline__ Jac<F> xyzz_to_jac_warp(const XYZZ<F>& p)
+{
+    if (xyzz_is_inf(p)) return {F::zero(), F::one(), F::zero()};
+    F s1[3];
+    { F a[3] = {p.ZZZ, p.ZZ, p.ZZ}; F b[3] = {p.ZZZ, p.ZZZ, p.ZZ}; warp_products<3>(s1, a, b); }
+    F zzz2 = s1[0], Z = s1[1], zz2 = s1[2];
+    F s2[2];
+    { F a[2] = {p.X, zz2}; F b[2] = {p.ZZ, p.ZZ}; warp_products<2>(s2, a, b); }
+    F s3[2];
+    { F a[2] = {s2[0], p.Y}; F b[2] = {zzz2, s2[1]}; warp_products<2>(s3, a, b); }
+    F s4[1];
+    { F a[1] = {s3[1]}; F b[1] = {zzz2}; warp_products<1>(s4, a, b); }
+    return {s3[0], s4[0], Z};
+}
+
 }  // namespace lzk

@@ -94,24 +94,30 @@ __global__ void k_dep_products(const Jac<Fq>* __restrict__ g1res, Scal r, Scal s
 
 // proof.A = a1 + A + r d1; proof.B = b2 + B2 + s d2;
 // proof.C = s a1 + r b1 + (r s) d1 + s A + r B1 + L + H
+// One warp per proof point (<<<1, 96>>>), warp-uniform additions: the
+// assembly ends every proof, so its chain of additions is on the critical
+// path.
 __global__ void k_assemble(const Aff<Fq>* g1c, const Aff<Fq2>* g2c, const Jac<Fq>* g1res, const Jac<Fq2>* g2res,
                            const XYZZ<Fq>* sm1, const XYZZ<Fq2>* sm2, lzk_groth16_proof* proof)
 {
-    uint32_t t = threadIdx.x;
-    if (t == 0) {
-        XYZZ<Fq> A = xyzz_add_cold(xyzz_add_cold(xyzz_from_aff(g1c[0]), jac_to_xyzz(g1res[0])), sm1[0]);
-        st_elem(reinterpret_cast<Jac<Fq>*>(&proof->A), xyzz_to_jac(A));
-    } else if (t == 1) {
-        XYZZ<Fq> C = xyzz_add_cold(sm1[1], sm1[2]);
-        C = xyzz_add_cold(C, sm1[3]);
-        C = xyzz_add_cold(C, sm1[4]);
-        C = xyzz_add_cold(C, sm1[5]);
-        C = xyzz_add_cold(C, jac_to_xyzz(g1res[2]));
-        C = xyzz_add_cold(C, jac_to_xyzz(g1res[3]));
-        st_elem(reinterpret_cast<Jac<Fq>*>(&proof->C), xyzz_to_jac(C));
-    } else if (t == 2) {
-        XYZZ<Fq2> B = xyzz_add_cold(xyzz_add_cold(xyzz_from_aff(g2c[0]), jac_to_xyzz(g2res[0])), sm2[0]);
-        st_elem(reinterpret_cast<Jac<Fq2>*>(&proof->B), xyzz_to_jac(B));
+    const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (w == 0) {
+        XYZZ<Fq> A = xyzz_add_warp(xyzz_add_warp(xyzz_from_aff(g1c[0]), jac_to_xyzz(g1res[0])), sm1[0]);
+        Jac<Fq> j = xyzz_to_jac_warp(A);
+        if (lane == 0) st_elem(reinterpret_cast<Jac<Fq>*>(&proof->A), j);
+    } else if (w == 1) {
+        XYZZ<Fq> C = xyzz_add_warp(sm1[1], sm1[2]);
+        C = xyzz_add_warp(C, sm1[3]);
+        C = xyzz_add_warp(C, sm1[4]);
+        C = xyzz_add_warp(C, sm1[5]);
+        C = xyzz_add_warp(C, jac_to_xyzz(g1res[2]));
+        C = xyzz_add_warp(C, jac_to_xyzz(g1res[3]));
+        Jac<Fq> j = xyzz_to_jac_warp(C);
+        if (lane == 0) st_elem(reinterpret_cast<Jac<Fq>*>(&proof->C), j);
+    } else if (w == 2) {
+        XYZZ<Fq2> B = xyzz_add_warp(xyzz_add_warp(xyzz_from_aff(g2c[0]), jac_to_xyzz(g2res[0])), sm2[0]);
+        Jac<Fq2> j = xyzz_to_jac_warp(B);
+        if (lane == 0) st_elem(reinterpret_cast<Jac<Fq2>*>(&proof->B), j);
     }
 }
 
@@ -395,7 +401,7 @@ int prove_ctx(const lzk_prover* p, ProveCtx* x, const Fr* z, const lzk_fr_t* r, 
     LZK_CUDA(cudaStreamWaitEvent(st, x->ev_s2, 0));
     LZK_CUDA(cudaStreamWaitEvent(st, x->ev_s3, 0));
     void* tr_as = trace_begin("groth16_assemble", st);
-    k_assemble<<<1, 32, 0, st>>>(p->g1c, p->g2c, x->g1res, x->g2res, x->sm1, x->sm2, proof); note_launch();
+    k_assemble<<<1, 96, 0, st>>>(p->g1c, p->g2c, x->g1res, x->g2res, x->sm1, x->sm2, proof); note_launch();
     trace_end(tr_as, st);
     trace_end(tr, st);
     return launch_status();

@@ -264,8 +264,8 @@ __device__ __forceinline__ XYZZ<F> shfl_pt(const XYZZ<F>& x, uint32_t lane)
 //   k_red_scale    one warp per sum: fold its partials, double it
 //                  i + log L times;
 //   k_red_combine  one warp per set: add the scaled sums.
-// For m = 2^16 the longest chain is 10 + 5 + 6 + 15 doublings + 5 dependent
-// point operations (a ladder of segment levels with the weights carried by
+// For m = 2^16 the longest chain is 10 + 5 + 6 + 15 doublings (warp-uniform,
+// xyzz_dbl_warp) + 5 dependent point operations (a ladder of segment levels with the weights carried by
 // doublings at every level needs about twice that), and every operation is a
 // latency-staged one (xyzz_add_cold / xyzz_dbl_cold).  Empty buckets
 // (off[k] == off[k+1]) read as the point at infinity.
@@ -352,11 +352,13 @@ __global__ void __launch_bounds__(128) k_red_scale(const XYZZ<F>* __restrict__ p
         XYZZ<F> x = xyzz_inf<F>();
         for (uint32_t c = lane; c < cnt; c += 32) x = xyzz_add_cold(x, ld_elem(src + c));
         for (uint32_t d = 16; d > 0; d >>= 1) x = xyzz_add_cold(x, shfl_xor_pt(x, d));
-        if (lane == 0) {
-            uint32_t dbls = s == 0 ? 0 : s - 1 + sh.lgL;
-            for (uint32_t d = 0; d < dbls; d++) x = xyzz_dbl_cold(x);
-            st_elem(scaled + g, x);
-        }
+        // lanes may hold different representations of the sum (an addition
+        // with swapped operands negates Y and ZZZ); the warp-uniform
+        // doublings need one
+        x = shfl_pt(x, 0);
+        uint32_t dbls = s == 0 ? 0 : s - 1 + sh.lgL;
+        for (uint32_t d = 0; d < dbls; d++) x = xyzz_dbl_warp(x);
+        if (lane == 0) st_elem(scaled + g, x);
     }
 }
 
@@ -387,17 +389,21 @@ int reduce_buckets(const XYZZ<F>* bsum, const uint32_t* off, uint32_t wb, uint32
     return launch_status();
 }
 
+// Horner over the bucket sets' weighted sums (plain bases), or the
+// conversion of the one set's sum (shifted-copy table): one warp, with
+// warp-uniform point operations.  Launched as <<<1, 32>>>.
 template <class F>
 __global__ void k_finish(const XYZZ<F>* __restrict__ win, uint32_t windows, uint32_t c, Jac<F>* out)
 {
-    if (gtid() != 0) return;
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
     XYZZ<F> r = xyzz_inf<F>();
     for (int w = (int)windows - 1; w >= 0; w--) {
         if (w != (int)windows - 1)
-            for (uint32_t d = 0; d < c; d++) r = xyzz_dbl_cold(r);
-        r = xyzz_add_cold(r, ld_elem(win + w));
+            for (uint32_t d = 0; d < c; d++) r = xyzz_dbl_warp(r);
+        r = xyzz_add_warp(r, ld_elem(win + w));
     }
-    st_elem(out, xyzz_to_jac(r));
+    Jac<F> j = xyzz_to_jac_warp(r);
+    if (threadIdx.x == 0) st_elem(out, j);
 }
 
 template <class F>
