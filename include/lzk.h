@@ -377,6 +377,12 @@ int lzk_msm_set_window(int group, uint32_t log_n, uint32_t window_bits);
  * Replaces the reference's synchronising Timer/CUDA_DEBUG pairs
  * (timer.cu:3-16, device-utils.cuh:3). */
 void lzk_trace_enable(int on);
+/* Restrict tracing to the comma-separated region names (NULL or "" = all
+ * regions).  Every traced region records two timing events in its stream,
+ * which costs a few microseconds of stream ordering each (about 1 % of a
+ * proof with every region traced), so throughput measurements trace only
+ * the regions they read. */
+int lzk_trace_only(const char* names);
 void lzk_trace_reset(void);
 /* Total device milliseconds and count of completed regions named `name`
  * since the last reset (waits for pending regions). */

@@ -63,6 +63,7 @@ SIGNATURES = {
     "lzk_msm_set_window": (c_i, [c_i, c_u32, c_u32]),
     "lzk_trace_enable": (None, [c_i]),
     "lzk_trace_reset": (None, []),
+    "lzk_trace_only": (c_i, [ctypes.c_char_p]),
     "lzk_trace_get": (c_i, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64)]),
     "lzk_trace_timeline": (c_i, [c_p, c_sz, ctypes.POINTER(c_sz)]),
     "lzk_probe_imad_rate": (c_i, [ctypes.POINTER(ctypes.c_double)]),
@@ -155,6 +156,11 @@ def call(name, *args):
 
 def trace_enable(on=True):
     lib().lzk_trace_enable(1 if on else 0)
+
+
+def trace_only(names=None):
+    """trace only these region names (an iterable of str; None = all)"""
+    call("lzk_trace_only", ",".join(names).encode() if names else None)
 
 
 def trace_reset():

@@ -26,6 +26,10 @@ struct TraceSpan {
 
 static std::mutex g_tr_mu;
 static bool g_tr_on = false;
+// names recorded while tracing is on (empty: all); each traced region puts
+// two timing events in its stream, a few microseconds of stream ordering,
+// so a throughput measurement traces only the regions it reads
+static std::vector<std::string> g_tr_only;
 static std::vector<TraceRec> g_tr_pending;
 static std::map<std::string, std::pair<double, uint64_t>> g_tr_sum;
 // timeline: spans relative to the first region begun since the last reset
@@ -42,6 +46,14 @@ bool trace_on() { return g_tr_on; }
 void* trace_begin(const char* name, cudaStream_t st)
 {
     if (!g_tr_on) return nullptr;
+    {
+        std::lock_guard<std::mutex> g(g_tr_mu);
+        if (!g_tr_only.empty()) {
+            bool hit = false;
+            for (const auto& n : g_tr_only) hit = hit || n == name;
+            if (!hit) return nullptr;
+        }
+    }
     TraceRec* r = new TraceRec{name, nullptr, nullptr};
     cudaEventCreate(&r->a);
     cudaEventCreate(&r->b);
@@ -115,6 +127,24 @@ void lzk_trace_enable(int on)
 {
     std::lock_guard<std::mutex> g(g_tr_mu);
     g_tr_on = on != 0;
+}
+
+int lzk_trace_only(const char* names)
+{
+    std::lock_guard<std::mutex> g(g_tr_mu);
+    g_tr_only.clear();
+    if (!names) return LZK_OK;
+    std::string cur;
+    for (const char* c = names;; c++) {
+        if (*c == ',' || *c == 0) {
+            if (!cur.empty()) g_tr_only.push_back(cur);
+            cur.clear();
+            if (*c == 0) break;
+        } else {
+            cur.push_back(*c);
+        }
+    }
+    return LZK_OK;
 }
 
 void lzk_trace_reset(void)

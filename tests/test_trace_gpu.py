@@ -43,3 +43,29 @@ def test_proof_timeline(cuda):
     _capi.trace_reset()
     assert _capi.trace_timeline() == []
     prover.close()
+
+
+def test_trace_only_filter(cuda):
+    import torch
+
+    from liblightzk_b200 import _capi, device, groth16, synth
+    circ = synth.Circuit(9, seed=4, n_public=2, n_free=32, block=32)
+    z = circ.witness(5)
+    pk = synth.ProvingKey(circ, seed=6)
+    prover = groth16.Prover(circ, pk, mode=groth16.STANDARD, window_bits=8)
+    r = device.to_host(synth.random_fr(2, 7, 1))
+    _capi.trace_reset()
+    _capi.trace_only(["msm_g1_accumulate", "groth16_assemble"])
+    _capi.trace_enable(True)
+    try:
+        prover.prove(z, r[0], r[1])
+        torch.cuda.synchronize()
+    finally:
+        _capi.trace_enable(False)
+        _capi.trace_only(None)
+    assert _capi.trace_get("msm_g1_accumulate")[1] == 4
+    assert _capi.trace_get("groth16_assemble")[1] == 1
+    assert _capi.trace_get("msm_g2")[1] == 0 and _capi.trace_get("groth16_prove")[1] == 0
+    assert {t[0] for t in _capi.trace_timeline()} == {"msm_g1_accumulate", "groth16_assemble"}
+    _capi.trace_reset()
+    prover.close()
