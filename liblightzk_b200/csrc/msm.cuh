@@ -251,56 +251,75 @@ __device__ __forceinline__ XYZZ<F> shfl_pt(const XYZZ<F>& x, uint32_t lane)
 // ---------------------------- bucket reduction ----------------------------
 // Per bucket set (one per window for plain bases, one for all windows with a
 // shifted-copy table) of m = 2^(c-1) buckets B_0..B_{m-1}, bucket k holding
-// digit k + 1, the weighted sum W = sum_k (k+1) B_k.  With tiles of
-// L = min(m, 32) buckets and P = m / L tiles,
+// digit k + 1, the weighted sum W = sum_k (k+1) B_k.  With tiles of L
+// buckets and P = m / L tiles,
 //   W = sum_u t_u + L sum_u u R_u = T + sum_{i < log P} 2^(i + log L) G_i,
 // where R_u is the sum of tile u, t_u = sum_j (j+1) B_{uL+j} its locally
 // weighted sum, T = sum_u t_u and G_i = sum of the R_u with bit i of u set
 // (bit slices of the tile index).  Four launches:
-//   k_red_tile     one warp per tile: shuffle suffix scan S_j = sum_{j'>=j}
-//                  B_{uL+j'}, R_u = S_0, t_u = sum_j S_j;
+//   k_red_tile     one warp per tile (below);
 //   k_red_slices   one warp per 32 members of one of the 1 + log P sums T,
 //                  G_0, G_1, ... (xor-shuffle tree);
 //   k_red_scale    one warp per sum: fold its partials, double it
-//                  i + log L times;
+//                  i + log L times (warp-uniform doublings);
 //   k_red_combine  one warp per set: add the scaled sums.
-// For m = 2^16 the longest chain is 10 + 5 + 6 + 15 doublings (warp-uniform,
-// xyzz_dbl_warp) + 5 dependent point operations (a ladder of segment levels with the weights carried by
-// doublings at every level needs about twice that), and every operation is a
-// latency-staged one (xyzz_add_cold / xyzz_dbl_cold).  Empty buckets
+// For m = 2^16 the longest chain is 19 + 5 + 6 + 15 doublings + 5 dependent
+// point operations; a ladder of 32-bucket levels with the weights carried by
+// doublings at every level needs about twice that.  Empty buckets
 // (off[k] == off[k+1]) read as the point at infinity.
+//
+// k_red_tile: lane j of a tile holds the run of r consecutive buckets
+// jr .. jr + r - 1 (r = 4 for m >= 128, L = 32 r; smaller sets take r = 2 or
+// 1 and L = m).  The lane forms the run's sum s_j and its locally weighted
+// sum t_j = sum_i (i+1) B_{jr+i} by running sums (two additions per
+// bucket), a shuffle suffix scan gives S_j = sum_{j'>=j} s_j', and since the
+// tile-local weight of bucket jr + i is jr + i + 1,
+//   R_u = S_0,   t_u = sum_j (t_j + r [j >= 1] S_j).
+// About 4.75 additions per bucket for r = 4, against 10 for a warp scan over
+// single buckets (r = 1).
 template <class F>
 __global__ void __launch_bounds__(128) k_red_tile(const XYZZ<F>* __restrict__ bsum, const uint32_t* __restrict__ off,
-                                                  uint32_t wb, uint32_t m, uint32_t L, XYZZ<F>* __restrict__ R,
-                                                  XYZZ<F>* __restrict__ T)
+                                                  uint32_t wb, uint32_t m, uint32_t L, uint32_t r,
+                                                  XYZZ<F>* __restrict__ R, XYZZ<F>* __restrict__ T)
 {
     const uint32_t lane = threadIdx.x & 31;
+    const uint32_t nl = L / r;   // active lanes
     const uint64_t total = (uint64_t)wb * (m / L);
     for (uint64_t tile = gtid() >> 5; tile < total; tile += gstride() >> 5) {
-        size_t k = (size_t)tile * L + lane;   // = w m + u L + lane
-        XYZZ<F> S = xyzz_inf<F>();
-        if (lane < L && off[k] != off[k + 1]) S = ld_elem(bsum + k);
-        for (uint32_t d = 1; d < L; d <<= 1) {
-            XYZZ<F> o = shfl_down_pt(S, d);
-            if (lane + d < L) S = xyzz_add_cold(S, o);
+        XYZZ<F> s = xyzz_inf<F>(), t = xyzz_inf<F>();
+        if (lane < nl) {
+            const size_t k0 = (size_t)tile * L + (size_t)lane * r;   // = w m + u L + j r
+            for (int i = (int)r - 1; i >= 0; i--) {
+                size_t k = k0 + (uint32_t)i;
+                if (off[k] != off[k + 1]) s = xyzz_add_cold(s, ld_elem(bsum + k));
+                t = xyzz_add_cold(t, s);
+            }
         }
-        XYZZ<F> t = S;
-        for (uint32_t d = L >> 1; d > 0; d >>= 1) t = xyzz_add_cold(t, shfl_xor_pt(t, d));
+        XYZZ<F> S = s;
+        for (uint32_t d = 1; d < nl; d <<= 1) {
+            XYZZ<F> o = shfl_down_pt(S, d);
+            if (lane + d < nl) S = xyzz_add_cold(S, o);
+        }
+        XYZZ<F> U = (lane >= 1 && lane < nl) ? S : xyzz_inf<F>();
+        for (uint32_t q = r; q > 1; q >>= 1) U = xyzz_dbl_cold(U);
+        XYZZ<F> V = xyzz_add_cold(t, U);
+        for (uint32_t d = nl >> 1; d > 0; d >>= 1) V = xyzz_add_cold(V, shfl_xor_pt(V, d));
         if (lane == 0) {
             st_elem(R + tile, S);
-            st_elem(T + tile, t);
+            st_elem(T + tile, V);
         }
     }
 }
 
 struct RedShape {
-    uint32_t L, lgL, P, lg;   // tile size, log2 L, tiles per set, log2 P
-    uint32_t cT, cG, NP, NS;  // chunks of T, chunks of each G_i, partials and sums per set
+    uint32_t r, L, lgL, P, lg;   // buckets per lane run, tile size, log2 L, tiles per set, log2 P
+    uint32_t cT, cG, NP, NS;     // chunks of T, chunks of each G_i, partials and sums per set
 };
 inline RedShape red_shape(uint32_t m)
 {
     RedShape s;
-    s.L = m < 32 ? m : 32;
+    s.r = m >= 128 ? 4 : m >= 64 ? 2 : 1;
+    s.L = m < 32 * s.r ? m : 32 * s.r;
     s.lgL = 0; while ((1u << s.lgL) < s.L) s.lgL++;
     s.P = m / s.L;
     s.lg = 0; while ((1u << s.lg) < s.P) s.lg++;
@@ -375,14 +394,14 @@ __global__ void __launch_bounds__(128) k_red_combine(const XYZZ<F>* __restrict__
 }
 
 // W_w of wb sets of m buckets (bsum / off indexed w m + k) into win[0..wb).
-// Scratch: R, T of wb * max(1, m / 32) points each; part and scaled fit in
-// the same size (NP, NS <= P).  win may alias R.
+// Scratch: R, T of at least wb * P points each (P <= max(1, m / 32)); part
+// and scaled fit in the same size (NP, NS <= P).  win may alias R.
 template <class F>
 int reduce_buckets(const XYZZ<F>* bsum, const uint32_t* off, uint32_t wb, uint32_t m, XYZZ<F>* R, XYZZ<F>* T,
                    XYZZ<F>* part, XYZZ<F>* scaled, XYZZ<F>* win, cudaStream_t st)
 {
     RedShape sh = red_shape(m);
-    k_red_tile<F><<<grid_for((size_t)wb * sh.P * 32, 128), 128, 0, st>>>(bsum, off, wb, m, sh.L, R, T); note_launch();
+    k_red_tile<F><<<grid_for((size_t)wb * sh.P * 32, 128), 128, 0, st>>>(bsum, off, wb, m, sh.L, sh.r, R, T); note_launch();
     k_red_slices<F><<<grid_for((size_t)wb * sh.NP * 32, 128), 128, 0, st>>>(R, T, wb, sh, part); note_launch();
     k_red_scale<F><<<grid_for((size_t)wb * sh.NS * 32, 128), 128, 0, st>>>(part, wb, sh, scaled); note_launch();
     k_red_combine<F><<<grid_for((size_t)wb * 32, 128), 128, 0, st>>>(scaled, wb, sh.NS, win); note_launch();
