@@ -686,8 +686,9 @@ def main():
     imad_peak = _capi.probe_imad_rate()
     W = msm.windows_for(args.window)
     nl = circ.n_vars - circ.n_public - 1
+    # G1 accumulation launches per proof: A, B1, and L + H as one MSM
     g1_points_per_proof = 2 * circ.n_vars + nl + (M - 1)
-    g1_launches_per_proof = 4
+    g1_launches_per_proof = 3
     avg_pts = g1_points_per_proof / g1_launches_per_proof
     alg_imad = avg_pts * W * FP_MUL_PER_G1_MADD * IMAD_PER_FP_MUL
     acc_avg_ms = acc_ms / max(acc_n, 1)
@@ -696,7 +697,10 @@ def main():
     prof = os.path.join(ROOT, "profiles", "msm_g1_accumulate_traffic.json")
     if os.path.exists(prof):
         try:
-            traffic = json.load(open(prof)).get("bytes_per_launch_at_2e20")
+            tj = json.load(open(prof))
+            # per average launch of this proof, scaled by its points from the
+            # captured launch (traffic grows with the entries)
+            traffic = tj["bytes_per_launch_at_2e20"] * avg_pts / tj.get("points_at_2e20", 1052674)
         except Exception:
             traffic = None
 
@@ -750,8 +754,9 @@ def main():
                      "traffic": traffic, "peak_source": "measured (lzk_probe_imad_rate, mad.lo/madc.hi chains)",
                      "algorithmic_imad_per_launch": alg_imad, "avg_launch_ms": acc_avg_ms,
                      "launches": acc_n,
-                     "timing": "CUDA events around each launch inside the timed proofs; the four G1 MSMs "
-                               "of a proof overlap on two streams, so a launch shares the GPU",
+                     "timing": "CUDA events around each launch inside the timed proofs; the three G1 MSMs "
+                               "of a proof (A, B1, and L + H as one) overlap on two streams, so a launch "
+                               "shares the GPU",
                      "isolated": iso_line},
         # sums of per-call device times (a separate traced pass of 3 proofs);
         # calls on different streams overlap

@@ -5,8 +5,8 @@
 // MSM tables (built once, resident in HBM) and all scratch, so a prove is a
 // fixed sequence of launches on three streams with no host round trip:
 //
-//   stream main : SpMV A z, B z, C z -> H polynomial -> H MSM -> assembly
-//   stream s1   : A MSM, B1 MSM, L MSM
+//   stream main : SpMV A z, B z, C z -> H polynomial -> L + H MSM -> assembly
+//   stream s1   : A MSM, B1 MSM
 //   stream s2   : B2 MSM (G2)
 //   stream s3   : fixed-point products r d1, s a1, r b1, (r s) d1, s d2 from
 //                 comb tables; after B1: s*A and r*B1 (variable base)
@@ -50,25 +50,6 @@ __device__ __forceinline__ Fr canon(const Scal& s)
     return from_mont(m);
 }
 
-// k * P, 4-bit fixed window: 15 precomputed multiples, then per nibble four
-// doublings and one addition (curve_utils.cuh:28-49 computes the same
-// product bit by bit)
-template <class F>
-__device__ XYZZ<F> smul_w4(const XYZZ<F>& P, const Fr& k)
-{
-    XYZZ<F> tab[16];
-    tab[0] = xyzz_inf<F>();
-    tab[1] = P;
-    for (int i = 2; i < 16; i++) tab[i] = (i & 1) ? xyzz_add_cold(tab[i - 1], P) : xyzz_dbl_cold(tab[i >> 1]);
-    XYZZ<F> acc = xyzz_inf<F>();
-    for (int w = 63; w >= 0; w--) {
-        for (int d = 0; d < 4; d++) acc = xyzz_dbl_cold(acc);
-        uint32_t nib = (k.v[w >> 3] >> (4 * (w & 7))) & 15u;
-        if (nib) acc = xyzz_add_cold(acc, tab[nib]);
-    }
-    return acc;
-}
-
 // fixed-base products from comb tables: thread 0 r d1, 1 s a1, 2 r b1,
 // 3 (r s) d1, 4 s d2
 __global__ void k_fixed_products(const Aff<Fq>* __restrict__ comb1, const Aff<Fq2>* __restrict__ comb2, Scal r, Scal s,
@@ -84,12 +65,33 @@ __global__ void k_fixed_products(const Aff<Fq>* __restrict__ comb1, const Aff<Fq
     sm1[t] = comb_mul(comb1 + table[t] * 8192, from_mont(k));
 }
 
-// variable-base products: thread 0 s * A, thread 1 r * B1
+// k * P, 4-bit fixed window: 15 precomputed multiples, then per nibble four
+// doublings and one addition (curve_utils.cuh:28-49 computes the same
+// product bit by bit).  Run by a whole warp with warp-uniform point
+// operations: every lane holds P, k and the table, and gets the product.
+template <class F>
+__device__ XYZZ<F> smul_w4_warp(const XYZZ<F>& P, const Fr& k)
+{
+    XYZZ<F> tab[16];
+    tab[0] = xyzz_inf<F>();
+    tab[1] = P;
+    for (int i = 2; i < 16; i++) tab[i] = (i & 1) ? xyzz_add_warp(tab[i - 1], P) : xyzz_dbl_warp(tab[i >> 1]);
+    XYZZ<F> acc = xyzz_inf<F>();
+    for (int w = 63; w >= 0; w--) {
+        for (int d = 0; d < 4; d++) acc = xyzz_dbl_warp(acc);
+        uint32_t nib = (k.v[w >> 3] >> (4 * (w & 7))) & 15u;
+        if (nib) acc = xyzz_add_warp(acc, tab[nib]);
+    }
+    return acc;
+}
+
+// variable-base products: warp 0 s * A, warp 1 r * B1 (<<<1, 64>>>)
 __global__ void k_dep_products(const Jac<Fq>* __restrict__ g1res, Scal r, Scal s, XYZZ<Fq>* __restrict__ sm1)
 {
-    uint32_t t = threadIdx.x;
-    if (t > 1) return;
-    sm1[4 + t] = smul_w4(jac_to_xyzz(g1res[t]), canon(t == 0 ? s : r));
+    const uint32_t w = threadIdx.x >> 5;
+    if (w > 1) return;
+    XYZZ<Fq> x = smul_w4_warp(jac_to_xyzz(g1res[w]), canon(w == 0 ? s : r));
+    if ((threadIdx.x & 31) == 0) sm1[4 + w] = x;
 }
 
 // proof.A = a1 + A + r d1; proof.B = b2 + B2 + s d2;
@@ -110,8 +112,7 @@ __global__ void k_assemble(const Aff<Fq>* g1c, const Aff<Fq2>* g2c, const Jac<Fq
         C = xyzz_add_warp(C, sm1[3]);
         C = xyzz_add_warp(C, sm1[4]);
         C = xyzz_add_warp(C, sm1[5]);
-        C = xyzz_add_warp(C, jac_to_xyzz(g1res[2]));
-        C = xyzz_add_warp(C, jac_to_xyzz(g1res[3]));
+        C = xyzz_add_warp(C, jac_to_xyzz(g1res[2]));   // L + H
         Jac<Fq> j = xyzz_to_jac_warp(C);
         if (lane == 0) st_elem(reinterpret_cast<Jac<Fq>*>(&proof->C), j);
     } else if (w == 2) {
@@ -194,9 +195,10 @@ int ctx_create(const lzk_prover* p, bool serving, ProveCtx** out)
             cfg.window_bits = p->c;
             cfg.flags = LZK_MSM_PRECOMPUTED;
             cfg.precomp_windows = p->wins;
-            size_t mx = p->M > p->n_vars ? p->M : p->n_vars;
-            cfg.level_stride = mx;
-            x->wsb[i] = lzk_msm_workspace_bytes(i == 2 ? 2 : 1, mx, &cfg);
+            // ws[0]: the concatenated L and H MSM; ws[1]: A and B1; ws[2]: B2
+            size_t n = i == 0 ? p->tn[2] : p->n_vars;
+            cfg.level_stride = n;
+            x->wsb[i] = lzk_msm_workspace_bytes(i == 2 ? 2 : 1, n, &cfg);
             rc = dalloc(&x->bytes, reinterpret_cast<char**>(&x->ws[i]), x->wsb[i]);
         }
         if (rc) break;
@@ -256,19 +258,29 @@ static int create(const lzk_groth16_circuit* c, const lzk_groth16_pk* pk, int mo
     p->c = window_bits ? window_bits : 17;
     if (p->c < 2 || p->c > 24) return LZK_EINVAL;
     p->wins = windows_for(p->c);
+    // level strides of the tables (ctx_create sizes the MSM workspaces by them)
+    p->tn[0] = p->tn[1] = c->n_vars;
+    p->nl = c->n_vars - c->n_public - 1;
+    p->tn[2] = p->nl + (p->M - 1);
 
     LZK_TRY(ctx_create(p, false, &p->ctx0));
     cudaStream_t st = p->ctx0->s1;
 
-    // tables
-    const lzk_g1_affine_t* q1[4] = {pk->a_query, pk->b1_query, pk->l_query, pk->h_query};
-    size_t n1[4] = {c->n_vars, c->n_vars, c->n_vars - c->n_public - 1, p->M - 1};
-    for (int q = 0; q < 4; q++) {
-        p->tn[q] = n1[q];
-        LZK_TRY(dalloc(&p->bytes, &p->tab[q], (size_t)p->wins * (n1[q] ? n1[q] : 1)));
-        if (n1[q])
-            LZK_TRY(lzk_g1_precompute(q1[q], n1[q], p->c, p->wins, reinterpret_cast<lzk_g1_affine_t*>(p->tab[q]), n1[q], st));
+    // tables: a and b1 (level stride n_vars); l and h concatenated in one
+    // table of level stride n_l + M - 1, since the L and H MSMs enter the
+    // proof only through their sum and run as one MSM
+    const lzk_g1_affine_t* q1[2] = {pk->a_query, pk->b1_query};
+    for (int q = 0; q < 2; q++) {
+        LZK_TRY(dalloc(&p->bytes, &p->tab[q], (size_t)p->wins * p->tn[q]));
+        LZK_TRY(lzk_g1_precompute(q1[q], p->tn[q], p->c, p->wins, reinterpret_cast<lzk_g1_affine_t*>(p->tab[q]),
+                                  p->tn[q], st));
     }
+    LZK_TRY(dalloc(&p->bytes, &p->tab[2], (size_t)p->wins * p->tn[2]));
+    if (p->nl)
+        LZK_TRY(lzk_g1_precompute(pk->l_query, p->nl, p->c, p->wins, reinterpret_cast<lzk_g1_affine_t*>(p->tab[2]),
+                                  p->tn[2], st));
+    LZK_TRY(lzk_g1_precompute(pk->h_query, p->M - 1, p->c, p->wins,
+                              reinterpret_cast<lzk_g1_affine_t*>(p->tab[2] + p->nl), p->tn[2], st));
     p->tn2 = c->n_vars;
     LZK_TRY(dalloc(&p->bytes, &p->tab2, (size_t)p->wins * p->tn2));
     LZK_TRY(lzk_g2_precompute(pk->b2_query, p->tn2, p->c, p->wins, reinterpret_cast<lzk_g2_affine_t*>(p->tab2), p->tn2, st));
@@ -354,11 +366,9 @@ int prove_ctx(const lzk_prover* p, ProveCtx* x, const Fr* z, const lzk_fr_t* r, 
     LZK_CUDA(cudaEventRecord(x->ev_b1, x->s1));
     LZK_CUDA(cudaStreamWaitEvent(x->s3, x->ev_b1, 0));
     void* tr_dep = trace_begin("groth16_dep_products", x->s3);
-    k_dep_products<<<1, 32, 0, x->s3>>>(x->g1res, rs, ss, x->sm1); note_launch();
+    k_dep_products<<<1, 64, 0, x->s3>>>(x->g1res, rs, ss, x->sm1); note_launch();
     trace_end(tr_dep, x->s3);
     LZK_CUDA(cudaEventRecord(x->ev_s3, x->s3));
-    size_t nl = p->n_vars - p->n_public - 1;
-    LZK_TRY(msm_tab1(p, x, 2, z + p->n_public + 1, nl, x->g1res + 2, 1, x->s1));
     LZK_CUDA(cudaEventRecord(x->ev_s1, x->s1));
 
     // main: H polynomial and H MSM
@@ -394,7 +404,18 @@ int prove_ctx(const lzk_prover* p, ProveCtx* x, const Fr* z, const lzk_fr_t* r, 
         hs = x0;
     }
     trace_end(tr_h, st);
-    LZK_TRY(msm_tab1(p, x, 3, hs, p->M - 1, x->g1res + 3, 0, st));
+    // L and H as one MSM: scalars z_(n_public+1) .. z_(n_vars-1), then the
+    // H coefficients, over the concatenated table
+    {
+        lzk_msm_cfg cfg{};
+        cfg.window_bits = p->c;
+        cfg.flags = LZK_MSM_PRECOMPUTED;
+        cfg.precomp_windows = p->wins;
+        cfg.level_stride = p->tn[2];
+        cfg.workspace = x->ws[0];
+        cfg.workspace_bytes = x->wsb[0];
+        LZK_TRY(msm_g1_concat(z + p->n_public + 1, p->nl, hs, p->M - 1, p->tab[2], x->g1res + 2, &cfg, st));
+    }
 
     // join and assemble
     LZK_CUDA(cudaStreamWaitEvent(st, x->ev_s1, 0));

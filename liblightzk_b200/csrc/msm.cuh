@@ -60,9 +60,10 @@ inline void plan_msm(MsmPlan& p, size_t n, uint32_t c, bool shared, size_t strid
 }
 
 // counting sort of the signed digits of all scalars into bucket lists:
-// cnt/off/ent as carved by plan_msm (msm_sort.cu)
+// cnt/off/ent as carved by plan_msm (msm_sort.cu).  With hi given, the
+// scalars are scalars[0..split) followed by hi[0..n - split).
 int msm_sort(const MsmPlan& p, const Fr* scalars, uint32_t* cnt, uint32_t* off, uint32_t* ent, uint32_t* bsums,
-             cudaStream_t st);
+             cudaStream_t st, const Fr* hi = nullptr, size_t split = 0);
 uint32_t msm_autotune(int group, size_t n, bool shared);
 
 // One digit sort shared by several shifted-table MSMs over the same scalars
@@ -78,6 +79,12 @@ int msm_g1_presorted(const Fr* scalars, const void* table, size_t n, Jac<Fq>* ou
                      cudaStream_t st, const uint32_t* off, const uint32_t* ent);
 int msm_g2_presorted(const Fr* scalars, const void* table, size_t n, Jac<Fq2>* out, const lzk_msm_cfg* cfg,
                      cudaStream_t st, const uint32_t* off, const uint32_t* ent);
+// A shifted-table G1 MSM whose scalars are two arrays, lo[0..n_lo) then
+// hi[0..n_hi), over one table of n_lo + n_hi points per level (msm_g1.cu):
+// two MSMs whose results are only ever added, done as one (one sort, one
+// bucket set, one reduction).  cfg must carry a workspace.
+int msm_g1_concat(const Fr* lo, size_t n_lo, const Fr* hi, size_t n_hi, const void* table, Jac<Fq>* out,
+                  const lzk_msm_cfg* cfg, cudaStream_t st);
 // exclusive scan of cnt[0..B) into off[0..B], off[B] = total; bsums holds
 // (B + 4095) / 4096 + 1 words (msm_sort.cu)
 int scan_offsets(const uint32_t* cnt, uint32_t B, uint32_t* off, uint32_t* bsums, cudaStream_t st);

@@ -11,6 +11,29 @@ int msm_g1_presorted(const Fr* scalars, const void* table, size_t n, Jac<Fq>* ou
     if (!cfg || !(cfg->flags & LZK_MSM_PRECOMPUTED) || !off || !ent) return LZK_EINVAL;
     return run_msm<G1>(scalars, table, n, out, cfg, st, cfg->window_bits, off, ent);
 }
+
+int msm_g1_concat(const Fr* lo, size_t n_lo, const Fr* hi, size_t n_hi, const void* table, Jac<Fq>* out,
+                  const lzk_msm_cfg* cfg, cudaStream_t st)
+{
+    size_t n = n_lo + n_hi;
+    if (!cfg || !(cfg->flags & LZK_MSM_PRECOMPUTED) || !cfg->workspace || !out || !table) return LZK_EINVAL;
+    if ((n_lo && !lo) || (n_hi && !hi) || n == 0 || n >= (1ull << 31)) return LZK_EINVAL;
+    uint32_t c = cfg->window_bits;
+    if (c < 2 || c > 24 || cfg->precomp_windows < windows_for(c) || cfg->level_stride < n) return LZK_EINVAL;
+    if ((size_t)windows_for(c) * cfg->level_stride >= (1ull << 31)) return LZK_EINVAL;
+    MsmPlan p;
+    plan_msm<G1>(p, n, c, true, cfg->level_stride);
+    if (cfg->workspace_bytes < p.bytes) return LZK_EINVAL;
+    // sort into the workspace at the offsets run_msm carves from it
+    char* base = static_cast<char*>(cfg->workspace);
+    uint32_t* off = reinterpret_cast<uint32_t*>(base + p.o_off);
+    uint32_t* ent = reinterpret_cast<uint32_t*>(base + p.o_ent);
+    void* tr = trace_begin("msm_g1_sort", st);
+    LZK_TRY(msm_sort(p, n_lo ? lo : hi, reinterpret_cast<uint32_t*>(base + p.o_cnt), off, ent,
+                     reinterpret_cast<uint32_t*>(base + p.o_scan), st, hi, n_lo));
+    trace_end(tr, st);
+    return run_msm<G1>(n_lo ? lo : hi, table, n, out, cfg, st, c, off, ent);
+}
 }  // namespace lzk
 
 extern "C" {

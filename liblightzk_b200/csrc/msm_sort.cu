@@ -64,11 +64,18 @@ struct DigitIter {
     }
 };
 
-__global__ void k_count(const Fr* __restrict__ scalars, size_t n, uint32_t c, uint32_t W, uint32_t nb,
-                        bool shared, uint32_t* __restrict__ cnt)
+// Scalar i of an MSM whose scalars are the concatenation of two arrays:
+// lo[0..split) then hi[0..n - split) (one array: split = n, hi unused).
+__device__ __forceinline__ const Fr* scalar_at(const Fr* lo, const Fr* hi, size_t split, uint64_t i)
+{
+    return i < split ? lo + i : hi + (i - split);
+}
+
+__global__ void k_count(const Fr* __restrict__ scalars, const Fr* __restrict__ hi, size_t split, size_t n, uint32_t c,
+                        uint32_t W, uint32_t nb, bool shared, uint32_t* __restrict__ cnt)
 {
     for (uint64_t i = gtid(); i < n; i += gstride()) {
-        DigitIter it; it.load(scalars + i);
+        DigitIter it; it.load(scalar_at(scalars, hi, split, i));
         for (uint32_t w = 0; w < W; w++) {
             bool neg; uint32_t d = it.next(w, c, neg);
             if (d) atomicAdd(cnt + (shared ? 0u : w * nb) + d - 1, 1u);
@@ -76,12 +83,12 @@ __global__ void k_count(const Fr* __restrict__ scalars, size_t n, uint32_t c, ui
     }
 }
 
-__global__ void k_scatter(const Fr* __restrict__ scalars, size_t n, uint32_t c, uint32_t W, uint32_t nb,
-                          bool shared, size_t stride, const uint32_t* __restrict__ off,
-                          uint32_t* __restrict__ cnt, uint32_t* __restrict__ ent)
+__global__ void k_scatter(const Fr* __restrict__ scalars, const Fr* __restrict__ hi, size_t split, size_t n,
+                          uint32_t c, uint32_t W, uint32_t nb, bool shared, size_t stride,
+                          const uint32_t* __restrict__ off, uint32_t* __restrict__ cnt, uint32_t* __restrict__ ent)
 {
     for (uint64_t i = gtid(); i < n; i += gstride()) {
-        DigitIter it; it.load(scalars + i);
+        DigitIter it; it.load(scalar_at(scalars, hi, split, i));
         for (uint32_t w = 0; w < W; w++) {
             bool neg; uint32_t d = it.next(w, c, neg);
             if (!d) continue;
@@ -164,16 +171,18 @@ int scan_offsets(const uint32_t* cnt, uint32_t B, uint32_t* off, uint32_t* bsums
 }
 
 int msm_sort(const MsmPlan& p, const Fr* scalars, uint32_t* cnt, uint32_t* off, uint32_t* ent, uint32_t* bsums,
-             cudaStream_t st)
+             cudaStream_t st, const Fr* hi, size_t split)
 {
+    if (!hi) split = p.n;
+    if (split > p.n) return LZK_EINVAL;
     LZK_CUDA(cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * p.B, st));
     unsigned g = grid_for(p.n, 256, 148 * 16);
-    k_count<<<g, 256, 0, st>>>(scalars, p.n, p.c, p.W, p.nb, p.shared, cnt); note_launch();
+    k_count<<<g, 256, 0, st>>>(scalars, hi, split, p.n, p.c, p.W, p.nb, p.shared, cnt); note_launch();
     uint32_t nblk = (p.B + kScanBlock - 1) / kScanBlock;
     k_scan_local<<<nblk, 1024, 0, st>>>(cnt, p.B, off, bsums); note_launch();
     k_scan_top<<<1, 1024, 0, st>>>(bsums, nblk, off, p.B); note_launch();
     k_scan_add<<<grid_for(p.B, 256, 148 * 8), 256, 0, st>>>(off, p.B, bsums); note_launch();
-    k_scatter<<<g, 256, 0, st>>>(scalars, p.n, p.c, p.W, p.nb, p.shared, p.stride, off, cnt, ent); note_launch();
+    k_scatter<<<g, 256, 0, st>>>(scalars, hi, split, p.n, p.c, p.W, p.nb, p.shared, p.stride, off, cnt, ent); note_launch();
     return launch_status();
 }
 

@@ -12,7 +12,7 @@ namespace lzk {
 // request, all sharing the prover's resident tables.
 struct ProveCtx {
     Fr* x = nullptr;                  // 3 * L: A z, B z, C z and the H polynomial
-    Jac<Fq>* g1res = nullptr;         // A, B1, L, H MSM results
+    Jac<Fq>* g1res = nullptr;         // A, B1 and L + H MSM results
     Jac<Fq2>* g2res = nullptr;        // B2 MSM result
     XYZZ<Fq>* sm1 = nullptr;          // r d1, s a1, r b1, (r s) d1, s A, r B1
     XYZZ<Fq2>* sm2 = nullptr;         // s d2
@@ -38,9 +38,11 @@ struct lzk_prover {
     uint64_t rows = 0, n_vars = 0, n_public = 0;
     uint32_t log_m = 0;
     size_t M = 0, L = 0;
-    // shifted-copy tables: a, b1, l, h (G1) and b2 (G2)
-    lzk::Aff<lzk::Fq>* tab[4] = {nullptr, nullptr, nullptr, nullptr};
-    size_t tn[4] = {0, 0, 0, 0};
+    // shifted-copy tables: a, b1, l and h concatenated (G1), b2 (G2); tn =
+    // level strides
+    lzk::Aff<lzk::Fq>* tab[3] = {nullptr, nullptr, nullptr};
+    size_t tn[3] = {0, 0, 0};
+    size_t nl = 0;          // points of the l query (n_vars - n_public - 1)
     lzk::Aff<lzk::Fq2>* tab2 = nullptr;
     size_t tn2 = 0;
     uint32_t c = 16, wins = 16;

@@ -26,7 +26,8 @@ def test_proof_timeline(cuda):
     finally:
         _capi.trace_enable(False)
     assert _capi.trace_get("groth16_prove")[1] == 1
-    assert _capi.trace_get("msm_g1")[1] == 4 and _capi.trace_get("msm_g2")[1] == 1
+    # G1 MSMs: A, B1, and L + H as one
+    assert _capi.trace_get("msm_g1")[1] == 3 and _capi.trace_get("msm_g2")[1] == 1
     tl = _capi.trace_timeline()
     names = [t[0] for t in tl]
     for n in ("groth16_prove", "groth16_h_poly", "groth16_fixed_products", "groth16_dep_products",
@@ -63,7 +64,7 @@ def test_trace_only_filter(cuda):
     finally:
         _capi.trace_enable(False)
         _capi.trace_only(None)
-    assert _capi.trace_get("msm_g1_accumulate")[1] == 4
+    assert _capi.trace_get("msm_g1_accumulate")[1] == 3
     assert _capi.trace_get("groth16_assemble")[1] == 1
     assert _capi.trace_get("msm_g2")[1] == 0 and _capi.trace_get("groth16_prove")[1] == 0
     assert {t[0] for t in _capi.trace_timeline()} == {"msm_g1_accumulate", "groth16_assemble"}
