@@ -7,7 +7,7 @@
 //
 //   stream main : SpMV A z, B z, C z -> H polynomial -> L + H MSM -> assembly
 //   stream s1   : A MSM, B1 MSM
-//   stream s2   : B2 MSM (G2)
+//   stream s2   : B2 MSM (G2), after the A MSM
 //   stream s3   : fixed-point products r d1, s a1, r b1, (r s) d1, s d2 from
 //                 comb tables; after B1: s*A and r*B1 (variable base)
 //
@@ -344,10 +344,16 @@ int prove_ctx(const lzk_prover* p, ProveCtx* x, const Fr* z, const lzk_fr_t* r, 
     // s1: one digit sort of z for the A, B1 and B2 MSMs (same scalars, same
     // window width, tables of the same level stride n_vars)
     LZK_TRY(msm_sort_scalars(z, p->n_vars, p->c, p->n_vars, x->zs_cnt, x->zs_off, x->zs_ent, x->zs_bsums, x->s1));
+
+    // s1: A and B1 MSMs; s3 picks up A and B1 for s*A and r*B1
+    LZK_TRY(msm_tab1(p, x, 0, z, p->n_vars, x->g1res + 0, 1, x->s1, true));
+
+    // s2: the G2 MSM, from the same sort, once the A MSM is done: started
+    // beside the A MSM its 2000-block accumulation kept the A MSM's fix-up
+    // and reduction waiting, which delayed B1 and the products that end the
+    // proof (measured 30.00 -> 29.73 ms per proof)
     LZK_CUDA(cudaEventRecord(x->ev_sorted, x->s1));
     LZK_CUDA(cudaStreamWaitEvent(x->s2, x->ev_sorted, 0));
-
-    // s2: the G2 MSM
     {
         lzk_msm_cfg cfg{};
         cfg.window_bits = p->c;
@@ -360,8 +366,6 @@ int prove_ctx(const lzk_prover* p, ProveCtx* x, const Fr* z, const lzk_fr_t* r, 
     }
     LZK_CUDA(cudaEventRecord(x->ev_s2, x->s2));
 
-    // s1: A, B1 and L MSMs; s3 picks up A and B1 for s*A and r*B1
-    LZK_TRY(msm_tab1(p, x, 0, z, p->n_vars, x->g1res + 0, 1, x->s1, true));
     LZK_TRY(msm_tab1(p, x, 1, z, p->n_vars, x->g1res + 1, 1, x->s1, true));
     LZK_CUDA(cudaEventRecord(x->ev_b1, x->s1));
     LZK_CUDA(cudaStreamWaitEvent(x->s3, x->ev_b1, 0));
@@ -371,7 +375,7 @@ int prove_ctx(const lzk_prover* p, ProveCtx* x, const Fr* z, const lzk_fr_t* r, 
     LZK_CUDA(cudaEventRecord(x->ev_s3, x->s3));
     LZK_CUDA(cudaEventRecord(x->ev_s1, x->s1));
 
-    // main: H polynomial and H MSM
+    // main: H polynomial, then the L + H MSM
     Fr* x0 = x->x;
     Fr* x1 = x->x + p->L;
     Fr* x2 = x->x + 2 * p->L;
