@@ -689,7 +689,12 @@ def main():
         return
 
     # ---------------- roofline of the dominant kernel ----------------
-    imad_peak = _capi.probe_imad_rate()
+    mad_chain_rate = _capi.probe_imad_rate()
+    mont_rate = _capi.probe_mont_rate()
+    # the roofline's denominator: Montgomery products per second in the
+    # kernels' own instruction form, counted in the IMAD-class unit of the
+    # algorithmic work (264 per product)
+    imad_peak = mont_rate * IMAD_PER_FP_MUL
     W = msm.windows_for(args.window)
     nl = circ.n_vars - circ.n_public - 1
     # G1 accumulation launches per proof: A, B1, and L + H as one MSM
@@ -757,7 +762,11 @@ def main():
         "roofline": {"kernel": "k_accumulate<Fq> (G1 bucket accumulation)", "bound": "int",
                      "achieved": achieved / 1e12 if achieved else None, "peak": imad_peak / 1e12,
                      "unit": "T IMAD/s", "frac": (achieved / imad_peak) if achieved else None,
-                     "traffic": traffic, "peak_source": "measured (lzk_probe_imad_rate, mad.lo/madc.hi chains)",
+                     "traffic": traffic,
+                     "peak_source": "measured: lzk_probe_mont_rate (independent Fq Montgomery products in the "
+                                    "kernels' instruction form, full occupancy) x 264 IMAD-class per product",
+                     "mont_products_per_s": mont_rate,
+                     "peak_mad_chains_T": mad_chain_rate / 1e12,
                      "algorithmic_imad_per_launch": alg_imad, "avg_launch_ms": acc_avg_ms,
                      "launches": acc_n,
                      "timing": "CUDA events around each launch inside the timed proofs; the three G1 MSMs "

@@ -55,6 +55,30 @@ const char* lzk_status_string(int status);
 /* Library version string. */
 const char* lzk_version(void);
 
+/* ---------------------------------------------------------- field ops
+ * Element-wise arithmetic on device arrays of n elements: out[i] = a[i] op
+ * b[i] (b unused by the unary ops).  Replaces the device mont_t operators
+ * (operator*, sqr, +=, -=, cneg, reciprocal, from/to Montgomery;
+ * mont_t.cuh:396-430, 208-302, 465-629) and fp2_t's (alt_bn128_t.cuh:
+ * 97-224) for code that works on whole vectors.  Elements are in Montgomery
+ * form (FROM_MONT returns the canonical integer, TO_MONT takes one); every
+ * result is canonical (< p).  The products go through the same device
+ * routines as the MSM, NTT and point formulas, so this is also how those
+ * routines are checked against host arithmetic.  INV of zero gives zero.
+ * out may alias a or b. */
+#define LZK_FIELD_FR  0
+#define LZK_FIELD_FQ  1
+#define LZK_FIELD_FQ2 2   /* elements are lzk_fq2_t */
+#define LZK_FOP_ADD       0
+#define LZK_FOP_SUB       1
+#define LZK_FOP_MUL       2
+#define LZK_FOP_SQR       3
+#define LZK_FOP_NEG       4
+#define LZK_FOP_INV       5
+#define LZK_FOP_FROM_MONT 6
+#define LZK_FOP_TO_MONT   7
+int lzk_field_op(int field, int op, const void* a, const void* b, void* out, size_t n, void* stream);
+
 /* ------------------------------------------------------------------ MSM
  * out = sum_i scalars[i] * bases[i], a Pippenger bucket method with signed
  * c-bit digits, counting-sorted bucket lists and XYZZ accumulation.
@@ -121,8 +145,13 @@ uint32_t lzk_msm_autotune_window(int group, size_t n, uint32_t flags);
  * process.  n may be at most LZK_MSM_NOALLOC_MAX_POINTS, and the scratch of
  * the chosen window (window_bits, 0 = autotuned) must fit; otherwise the call
  * returns LZK_EINVAL without queuing work.  The first call on each device
- * looks up the array's device address (cudaGetSymbolAddress), so make it
- * before beginning any stream capture.  All calls on a device share the
+ * (n = 0 is enough) also sets that device up: under CUDA's lazy module
+ * loading the MSM kernels are loaded, and their local memory sized, on
+ * first use, which can need device memory, so that call runs one small MSM
+ * entirely inside the array.  Make it before your allocator reserves the
+ * device's memory and before beginning any stream capture (or run with
+ * CUDA_MODULE_LOADING=EAGER); after a cudaDeviceReset the set-up is not
+ * repeated.  All calls on a device share the
  * array: the counters that must start at zero are cleared by every call, but
  * calls whose work overlaps on the GPU race -- order them. */
 #define LZK_MSM_NOALLOC_MAX_POINTS   65536u
@@ -403,6 +432,10 @@ uint64_t lzk_launch_count(void);
 /* Measured 32-bit integer multiply-add rate of the current device
  * (mad.lo/madc.hi operations per second); synchronous. */
 int lzk_probe_imad_rate(double* ops_per_s);
+/* Measured rate of Fq Montgomery products per second on the current device,
+ * in the instruction form the MSM and NTT kernels issue (independent
+ * products, full occupancy); synchronous. */
+int lzk_probe_mont_rate(double* products_per_s);
 
 #ifdef __cplusplus
 }

@@ -19,6 +19,7 @@ c_i = ctypes.c_int
 SIGNATURES = {
     "lzk_status_string": (ctypes.c_char_p, [c_i]),
     "lzk_version": (ctypes.c_char_p, []),
+    "lzk_field_op": (c_i, [c_i, c_i, c_p, c_p, c_p, c_sz, c_p]),
     "lzk_msm_g1": (c_i, [c_p, c_p, c_sz, c_p, c_p, c_p]),
     "lzk_msm_g2": (c_i, [c_p, c_p, c_sz, c_p, c_p, c_p]),
     "lzk_msm_g1_noalloc": (c_i, [c_p, c_p, c_sz, c_p, c_u32, c_p]),
@@ -67,6 +68,7 @@ SIGNATURES = {
     "lzk_trace_get": (c_i, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64)]),
     "lzk_trace_timeline": (c_i, [c_p, c_sz, ctypes.POINTER(c_sz)]),
     "lzk_probe_imad_rate": (c_i, [ctypes.POINTER(ctypes.c_double)]),
+    "lzk_probe_mont_rate": (c_i, [ctypes.POINTER(ctypes.c_double)]),
     "lzk_launch_count": (ctypes.c_uint64, []),
 }
 
@@ -191,6 +193,12 @@ def trace_timeline():
 def probe_imad_rate():
     r = ctypes.c_double()
     call("lzk_probe_imad_rate", ctypes.byref(r))
+    return r.value
+
+
+def probe_mont_rate():
+    r = ctypes.c_double()
+    call("lzk_probe_mont_rate", ctypes.byref(r))
     return r.value
 
 

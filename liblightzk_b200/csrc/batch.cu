@@ -135,7 +135,7 @@ static int run_plan(lzk_batch_plan* p, cudaStream_t st)
     using X = XYZZ<F>;
     uint32_t count = (uint32_t)p->msm.size();
     if (count && p->total_pts) {
-        unsigned g = grid_for(p->total_pts, 256, 148 * 16);
+        unsigned g = grid_for(p->total_pts, 256, sm_count() * 16);
         k_bgather<F><<<g, 256, 0, st>>>(p->d_desc, p->d_ptsoff, count, p->total_pts, static_cast<Aff<F>*>(p->bases)); note_launch();
         LZK_CUDA(cudaMemsetAsync(p->cnt, 0, sizeof(uint32_t) * p->total_buckets, st));
         k_bdigits<false><<<g, 256, 0, st>>>(p->d_desc, p->d_ptsoff, count, p->total_pts, p->off, p->cnt, p->ent); note_launch();
@@ -146,11 +146,11 @@ static int run_plan(lzk_batch_plan* p, cudaStream_t st)
             p->bases, p->ent, p->off, (uint32_t)p->total_buckets, p->chunks, bsum, static_cast<X*>(p->head),
             static_cast<X*>(p->tail)); note_launch();
         LZK_CUDA(cudaMemsetAsync(p->large, 0, sizeof(uint32_t), st));
-        k_fixup<F><<<grid_for(p->total_buckets, 256, 148 * 8), 256, 0, st>>>(p->off, (uint32_t)p->total_buckets, bsum,
+        k_fixup<F><<<grid_for(p->total_buckets, 256, sm_count() * 8), 256, 0, st>>>(p->off, (uint32_t)p->total_buckets, bsum,
                                                                             static_cast<X*>(p->head),
                                                                             static_cast<X*>(p->tail), p->large); note_launch();
         constexpr unsigned fx_threads = 32768 / sizeof(X);
-        k_fixup_large<F><<<148 * 2, fx_threads, fx_threads * sizeof(X), st>>>(p->off, bsum, static_cast<X*>(p->head),
+        k_fixup_large<F><<<sm_count() * 2, fx_threads, fx_threads * sizeof(X), st>>>(p->off, bsum, static_cast<X*>(p->head),
                                                                              static_cast<X*>(p->tail), p->large); note_launch();
         // one bucket reduction per window width
         uint64_t wdone = 0;

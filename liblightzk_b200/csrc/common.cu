@@ -1,5 +1,6 @@
 // common.cu -- status strings, version, device memory-pool policy.
 #include "common.cuh"
+#include <atomic>
 #include <mutex>
 
 namespace lzk {
@@ -19,6 +20,22 @@ void keep_pool_cached()
     }
     cudaGetLastError();
     done[dev] = true;
+}
+
+unsigned sm_count()
+{
+    static std::atomic<unsigned> cached[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) { cudaGetLastError(); return 128; }
+    unsigned v = cached[dev].load(std::memory_order_relaxed);
+    if (v) return v;
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) {
+        cudaGetLastError();
+        return 128;
+    }
+    cached[dev].store((unsigned)n, std::memory_order_relaxed);
+    return (unsigned)n;
 }
 
 }  // namespace lzk

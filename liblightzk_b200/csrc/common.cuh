@@ -49,6 +49,10 @@ void trace_end(void* h, cudaStream_t st);
 // stream-ordered scratch of repeated calls is served from the pool.
 void keep_pool_cached();
 
+// Streaming multiprocessors of the current device (queried once per device
+// and cached); grid-stride kernels size their grids in multiples of it.
+unsigned sm_count();
+
 // Scratch carved from a caller buffer or allocated stream-ordered from the
 // device pool (cudaMallocAsync / cudaFreeAsync on the same stream).
 struct Scratch {

@@ -395,7 +395,7 @@ int prove_ctx(const lzk_prover* p, ProveCtx* x, const Fr* z, const lzk_fr_t* r, 
     if (p->mode == LZK_PROVE_REFERENCE) {
         LZK_TRY(ntt_run(x->x, p->log_m, LZK_NTT_INVERSE, 3, p->L, nullptr, st));
         LZK_TRY(ntt_run(x->x, p->log_m + 1, LZK_NTT_FORWARD, 3, p->L, nullptr, st));
-        k_abc<<<grid_for(p->L, 256, 148 * 8), 256, 0, st>>>(x0, x1, x2, p->L, nullptr); note_launch();
+        k_abc<<<grid_for(p->L, 256, sm_count() * 8), 256, 0, st>>>(x0, x1, x2, p->L, nullptr); note_launch();
         NttTables t4; CosetTables ct;
         LZK_TRY(get_tables(p->log_m + 2, t4, ct));
         LZK_TRY(ntt_run(x0, p->log_m + 1, LZK_NTT_INVERSE, 1, 0, t4.consts + 2, st));
@@ -403,7 +403,7 @@ int prove_ctx(const lzk_prover* p, ProveCtx* x, const Fr* z, const lzk_fr_t* r, 
     } else {
         LZK_TRY(ntt_run(x->x, p->log_m, LZK_NTT_INVERSE, 3, p->L, nullptr, st));
         LZK_TRY(ntt_run(x->x, p->log_m, LZK_NTT_COSET_FORWARD, 3, p->L, nullptr, st));
-        k_abc<<<grid_for(p->L, 256, 148 * 8), 256, 0, st>>>(x0, x1, x2, p->L, p->zinv); note_launch();
+        k_abc<<<grid_for(p->L, 256, sm_count() * 8), 256, 0, st>>>(x0, x1, x2, p->L, p->zinv); note_launch();
         LZK_TRY(ntt_run(x0, p->log_m, LZK_NTT_COSET_INVERSE, 1, 0, nullptr, st));
         hs = x0;
     }
@@ -542,7 +542,7 @@ int lzk_poly_a_times_b_minus_c(lzk_fr_t* A, const lzk_fr_t* B, const lzk_fr_t* C
 {
     if (!n) return LZK_OK;
     if (!A || !B || !C) return LZK_EINVAL;
-    k_abc<<<grid_for(n, 256, 148 * 8), 256, 0, as_stream(stream)>>>(reinterpret_cast<Fr*>(A), reinterpret_cast<const Fr*>(B),
+    k_abc<<<grid_for(n, 256, sm_count() * 8), 256, 0, as_stream(stream)>>>(reinterpret_cast<Fr*>(A), reinterpret_cast<const Fr*>(B),
                                                                      reinterpret_cast<const Fr*>(C), n, nullptr); note_launch();
     return launch_status();
 }

@@ -210,7 +210,7 @@ int lzk_random_fr(uint64_t seed, uint64_t stream_id, uint64_t offset, size_t n, 
 {
     if (!n) return LZK_OK;
     if (!out) return LZK_EINVAL;
-    k_random_fr<<<grid_for(n, 256, 148 * 16), 256, 0, as_stream(stream)>>>(seed, stream_id, offset, n,
+    k_random_fr<<<grid_for(n, 256, sm_count() * 16), 256, 0, as_stream(stream)>>>(seed, stream_id, offset, n,
                                                                          reinterpret_cast<Fr*>(out)); note_launch();
     return launch_status();
 }

@@ -514,10 +514,10 @@ int run_msm(const Fr* scalars, const void* bases, size_t n, Jac<typename Gp::F>*
     trace_end(tr, st);
     void* tr_fix = trace_begin(sizeof(F) == 32 ? "msm_g1_fixup" : "msm_g2_fixup", st);
     LZK_CUDA(cudaMemsetAsync(large, 0, sizeof(uint32_t), st));
-    k_fixup<F><<<grid_for(p.B, 256, 148 * 8), 256, 0, st>>>(off, p.B, bsum, head, tail, large); note_launch();
+    k_fixup<F><<<grid_for(p.B, 256, sm_count() * 8), 256, 0, st>>>(off, p.B, bsum, head, tail, large); note_launch();
     {
         constexpr unsigned fx_threads = 32768 / sizeof(X);   // 32 KB of shared memory
-        k_fixup_large<F><<<148 * 2, fx_threads, fx_threads * sizeof(X), st>>>(off, bsum, head, tail, large); note_launch();
+        k_fixup_large<F><<<sm_count() * 2, fx_threads, fx_threads * sizeof(X), st>>>(off, bsum, head, tail, large); note_launch();
     }
     trace_end(tr_fix, st);
     LZK_TRY(launch_status());

@@ -19,10 +19,23 @@
 // streams without ordering between them) would race on the array.  Order
 // such calls, or use lzk_msm_g1 with separate workspaces.
 //
-// The device address of the array is looked up with cudaGetSymbolAddress the
-// first time each device is used (the array's name in host code is only a
-// stand-in and must never be handed to a kernel).  That first call per device
-// should therefore come before any stream capture is begun.
+// Set-up: the first call on each device (n = 0 is enough) prepares that
+// device before doing its own work.  Under CUDA's lazy module loading (the
+// default since CUDA 12.2) kernels are loaded, and their local memory is
+// sized, only when first used, and either may need device memory; a
+// process whose allocator takes the device's memory right after start-up
+// would then see the first MSM fail.  So the set-up runs one MSM of a
+// single zero scalar over an infinite base whose inputs, output and scratch
+// all lie in the array, on the caller's stream: every kernel the entry point
+// launches is then loaded and has run once.  Make that first call before
+// the allocator reserves its memory and before beginning any stream capture.
+// A cudaDeviceReset unloads everything again, and the set-up is not
+// repeated after one.
+//
+// The device address of the array is looked up with cudaGetSymbolAddress on
+// every call (the array's name in host code is only a stand-in and must
+// never be handed to a kernel); once the module is loaded the lookup is a
+// table read.
 #include "common.cuh"
 #include <mutex>
 
@@ -31,25 +44,45 @@ namespace lzk {
 static __device__ __align__(256) unsigned char g_msm_noalloc_scratch[LZK_MSM_NOALLOC_SCRATCH_BYTES];
 
 static std::mutex g_noalloc_mu;
-static void* g_noalloc_ptr[64] = {nullptr};
+static bool g_noalloc_ready[64] = {false};
 
 // device address of the scratch array on the current device
-static int noalloc_scratch(void** out)
+static int noalloc_scratch(void** out, int* dev_out)
 {
     int dev = 0;
     LZK_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) return LZK_EUNSUPPORTED;
-    std::lock_guard<std::mutex> g(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_msm_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            cudaGetLastError();
-            return LZK_EDEVICE;
-        }
-        g_noalloc_ptr[dev] = p;
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_msm_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        cudaGetLastError();
+        return LZK_EDEVICE;
     }
-    *out = g_noalloc_ptr[dev];
+    *out = p;
+    *dev_out = dev;
+    return LZK_OK;
+}
+
+// One-time set-up of the current device (see the file comment): an MSM of
+// n = 0 (the point-at-infinity path) and one of n = 1 with a zero scalar and
+// an infinite base, everything carved from the scratch array.  The first
+// kilobyte holds the inputs and outputs, the rest is the MSM's workspace.
+static int noalloc_setup(char* scratch, int dev, cudaStream_t st)
+{
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (g_noalloc_ready[dev]) return LZK_OK;
+    constexpr size_t kIo = 1024;
+    lzk_fr_t* s = reinterpret_cast<lzk_fr_t*>(scratch);
+    lzk_g1_affine_t* b = reinterpret_cast<lzk_g1_affine_t*>(scratch + 256);
+    lzk_g1_t* out = reinterpret_cast<lzk_g1_t*>(scratch + 512);
+    LZK_CUDA(cudaMemsetAsync(scratch, 0, kIo, st));
+    lzk_msm_cfg cfg = {};
+    cfg.window_bits = 2;
+    cfg.workspace = scratch + kIo;
+    cfg.workspace_bytes = LZK_MSM_NOALLOC_SCRATCH_BYTES - kIo;
+    LZK_TRY(lzk_msm_g1(s, b, 0, out, &cfg, st));
+    LZK_TRY(lzk_msm_g1(s, b, 1, out, &cfg, st));
+    g_noalloc_ready[dev] = true;
     return LZK_OK;
 }
 
@@ -68,7 +101,9 @@ int lzk_msm_g1_noalloc(const lzk_fr_t* scalars, const lzk_g1_affine_t* bases, si
     size_t need = lzk_msm_workspace_bytes(1, n, &cfg);
     if (need > LZK_MSM_NOALLOC_SCRATCH_BYTES) return LZK_EINVAL;
     void* scratch = nullptr;
-    LZK_TRY(noalloc_scratch(&scratch));
+    int dev = 0;
+    LZK_TRY(noalloc_scratch(&scratch, &dev));
+    LZK_TRY(noalloc_setup(static_cast<char*>(scratch), dev, as_stream(stream)));
     cfg.workspace = scratch;
     cfg.workspace_bytes = LZK_MSM_NOALLOC_SCRATCH_BYTES;
     return lzk_msm_g1(scalars, bases, n, out, &cfg, stream);

@@ -166,7 +166,7 @@ int scan_offsets(const uint32_t* cnt, uint32_t B, uint32_t* off, uint32_t* bsums
     if (nblk == 0) nblk = 1;
     k_scan_local<<<nblk, 1024, 0, st>>>(cnt, B, off, bsums); note_launch();
     k_scan_top<<<1, 1024, 0, st>>>(bsums, nblk, off, B); note_launch();
-    k_scan_add<<<grid_for(B, 256, 148 * 8), 256, 0, st>>>(off, B, bsums); note_launch();
+    k_scan_add<<<grid_for(B, 256, sm_count() * 8), 256, 0, st>>>(off, B, bsums); note_launch();
     return launch_status();
 }
 
@@ -176,12 +176,12 @@ int msm_sort(const MsmPlan& p, const Fr* scalars, uint32_t* cnt, uint32_t* off, 
     if (!hi) split = p.n;
     if (split > p.n) return LZK_EINVAL;
     LZK_CUDA(cudaMemsetAsync(cnt, 0, sizeof(uint32_t) * p.B, st));
-    unsigned g = grid_for(p.n, 256, 148 * 16);
+    unsigned g = grid_for(p.n, 256, sm_count() * 16);
     k_count<<<g, 256, 0, st>>>(scalars, hi, split, p.n, p.c, p.W, p.nb, p.shared, cnt); note_launch();
     uint32_t nblk = (p.B + kScanBlock - 1) / kScanBlock;
     k_scan_local<<<nblk, 1024, 0, st>>>(cnt, p.B, off, bsums); note_launch();
     k_scan_top<<<1, 1024, 0, st>>>(bsums, nblk, off, p.B); note_launch();
-    k_scan_add<<<grid_for(p.B, 256, 148 * 8), 256, 0, st>>>(off, p.B, bsums); note_launch();
+    k_scan_add<<<grid_for(p.B, 256, sm_count() * 8), 256, 0, st>>>(off, p.B, bsums); note_launch();
     k_scatter<<<g, 256, 0, st>>>(scalars, hi, split, p.n, p.c, p.W, p.nb, p.shared, p.stride, off, cnt, ent); note_launch();
     return launch_status();
 }

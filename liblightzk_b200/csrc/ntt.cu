@@ -264,7 +264,7 @@ static int ntt_enqueue(Fr* data, uint32_t k, uint32_t count, size_t bstride, con
         k_ntt_pass<<<dim3((unsigned)blocks, count), kNttThreads, smem, st>>>(data, pp, tw, flags, pre_lo, pre_hi, bstride, ptrs); note_launch();
         s0 += m;
     }
-    k_ntt_bitrev<<<dim3(grid_for(n, 256, 148 * 8), count), 256, 0, st>>>(data, k, scale, post_lo, post_hi, bstride, ptrs); note_launch();
+    k_ntt_bitrev<<<dim3(grid_for(n, 256, sm_count() * 8), count), 256, 0, st>>>(data, k, scale, post_lo, post_hi, bstride, ptrs); note_launch();
     return launch_status();
 }
 

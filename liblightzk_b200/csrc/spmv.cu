@@ -40,7 +40,7 @@ int lzk_spmv3(const lzk_csr* A, const lzk_csr* B, const lzk_csr* C, const lzk_fr
     uint64_t rows = a.rows > b.rows ? a.rows : b.rows;
     rows = rows > c.rows ? rows : c.rows;
     if (rows == 0) return LZK_OK;
-    k_spmv3<<<dim3(grid_for(rows, 256, 148 * 8), 3), 256, 0, as_stream(stream)>>>(
+    k_spmv3<<<dim3(grid_for(rows, 256, sm_count() * 8), 3), 256, 0, as_stream(stream)>>>(
         a, b, c, reinterpret_cast<const Fr*>(z), A ? reinterpret_cast<Fr*>(Az) : nullptr,
         B ? reinterpret_cast<Fr*>(Bz) : nullptr, C ? reinterpret_cast<Fr*>(Cz) : nullptr); note_launch();
     return launch_status();

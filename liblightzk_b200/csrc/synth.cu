@@ -76,7 +76,7 @@ int lzk_r1cs_check(const lzk_csr* A, const lzk_csr* B, const lzk_csr* C, const l
     rows = rows < c.rows ? rows : c.rows;
     LZK_CUDA(cudaMemsetAsync(bad_rows, 0, sizeof(unsigned long long), as_stream(stream)));
     if (!rows) return LZK_OK;
-    k_r1cs_check<<<grid_for(rows, 128, 148 * 8), 128, 0, as_stream(stream)>>>(a, b, c, reinterpret_cast<const Fr*>(z),
+    k_r1cs_check<<<grid_for(rows, 128, sm_count() * 8), 128, 0, as_stream(stream)>>>(a, b, c, reinterpret_cast<const Fr*>(z),
                                                                              rows, bad_rows); note_launch();
     return launch_status();
 }

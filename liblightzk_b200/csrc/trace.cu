@@ -6,6 +6,7 @@
 // every phase; here a traced region only records two events on its stream,
 // and durations are resolved when the host asks for them.
 #include "common.cuh"
+#include "field.cuh"
 #include <atomic>
 #include <map>
 #include <mutex>
@@ -115,6 +116,33 @@ __global__ void k_imad_probe(uint32_t iters, uint32_t seed, uint32_t* sink)
     if (acc == 0x12345678u) sink[0] = acc;
 }
 
+// Independent Montgomery products in the form the MSM and NTT kernels issue
+// (mul: mont_mul_core's wide products and 64-bit additions, then the final
+// conditional subtraction): each thread keeps kMontChains products in
+// flight, x_k <- x_k * y, so the rate is bound by the product's
+// instructions, not by a dependency chain.
+constexpr int kMontChains = 4;
+__global__ void __launch_bounds__(128) k_mont_probe(uint32_t iters, uint32_t seed, uint32_t* sink)
+{
+    Fq x[kMontChains], y;
+    uint32_t h = seed * 0x9e3779b9u ^ (uint32_t)gtid();
+    for (int i = 0; i < 8; i++) {
+        h = h * 1664525u + 1013904223u;
+        y.v[i] = h;
+        for (int k = 0; k < kMontChains; k++) x[k].v[i] = h ^ (0x85ebca6bu * (k + 1));
+    }
+    y.v[7] &= 0x0fffffffu;                       // operands below p
+    for (int k = 0; k < kMontChains; k++) x[k].v[7] &= 0x0fffffffu;
+    for (uint32_t it = 0; it < iters; it++) {
+        #pragma unroll
+        for (int k = 0; k < kMontChains; k++) x[k] = mul(x[k], y);
+    }
+    uint32_t acc = 0;
+    for (int k = 0; k < kMontChains; k++)
+        for (int i = 0; i < 8; i++) acc ^= x[k].v[i];
+    if (acc == 0x12345678u) sink[0] = acc;
+}
+
 }  // namespace lzk
 
 using namespace lzk;
@@ -212,6 +240,35 @@ int lzk_probe_imad_rate(double* ops_per_s)
     if (e != cudaSuccess) return cuda_status(e);
     double ops = (double)blocks * threads * iters * 8.0 * 4.0;
     *ops_per_s = ops / (ms * 1e-3);
+    return LZK_OK;
+}
+
+// Measured rate of Montgomery products (Fq, the instruction form of the
+// kernels' products) on this device at full occupancy.  Synchronous; ~0.1 s.
+int lzk_probe_mont_rate(double* products_per_s)
+{
+    if (!products_per_s) return LZK_EINVAL;
+    int per_sm = 0;
+    LZK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mont_probe, 128, 0));
+    if (per_sm <= 0) return LZK_EDEVICE;
+    uint32_t* sink;
+    LZK_CUDA(cudaMalloc(&sink, 4));
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const uint32_t iters = 2048, threads = 128, blocks = sm_count() * (uint32_t)per_sm * 4;
+    k_mont_probe<<<blocks, threads>>>(16, 1u, sink); note_launch();  // warm-up
+    cudaEventRecord(a);
+    k_mont_probe<<<blocks, threads>>>(iters, 1u, sink); note_launch();
+    cudaEventRecord(b);
+    cudaError_t e = cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(sink);
+    if (e != cudaSuccess) return cuda_status(e);
+    *products_per_s = (double)blocks * threads * iters * kMontChains / (ms * 1e-3);
     return LZK_OK;
 }
 
