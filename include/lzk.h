@@ -41,6 +41,7 @@ extern "C" {
 #define LZK_EBUSY        -6   /* busy: pending, or refused by the memory budget */
 #define LZK_ECANCELED    -7   /* request cancelled before it started */
 #define LZK_EREJECTED    -8   /* request can never fit the memory budget */
+#define LZK_EIO          -9   /* a file cannot be read or written, or is not a valid key file */
 
 typedef struct { uint64_t limb[4]; } lzk_fr_t;
 typedef struct { uint64_t limb[4]; } lzk_fq_t;
@@ -299,6 +300,35 @@ size_t lzk_prover_device_bytes(const lzk_prover* prover);
 int lzk_groth16_prove(lzk_prover* prover, const lzk_fr_t* z, const lzk_fr_t* r, const lzk_fr_t* s,
                       lzk_groth16_proof* proof, void* stream);
 
+/* Proving keys on disk.  The reference regenerates its key on every run
+ * from unseeded randomness (Groth16::Setup, groth16.cuh:48-152); a service
+ * saves each circuit's key once and loads it when it makes the circuit's
+ * prover (lzk_prover_create reads the key only while it builds its tables,
+ * so the loaded copy can be freed right after).
+ *
+ * File layout (little-endian, version 1): a 128-byte header -- magic
+ * "LZKG16PK", u32 version, u32 header size (128), u64 n_vars, u64 n_public,
+ * u32 log_domain, u32 0, u64 point counts of the a, b1, b2, l, h queries
+ * (n_vars, n_vars, n_vars, n_vars - n_public - 1, 2^log_domain - 1), u64
+ * checksum of the body, zeros -- then the body: alpha1, beta1, delta1 (G1
+ * affine), beta2, delta2 (G2 affine), and the five query arrays in that
+ * order.  Coordinates are the Montgomery limbs of the lzk_* types above.
+ *
+ * lzk_pk_save writes pk (query arrays in device memory) for a circuit of
+ * the given shape; lzk_pk_load checks the header, the sizes and the
+ * checksum (LZK_EIO on any mismatch, a missing or short file), copies the
+ * arrays into one device allocation owned by *out and fills *view (ready
+ * for lzk_prover_create) and *info (may be NULL).  Both are synchronous. */
+typedef struct lzk_pk_info {
+    uint64_t n_vars, n_public;
+    uint32_t log_domain;
+    uint32_t version;          /* filled by lzk_pk_load */
+} lzk_pk_info;
+typedef struct lzk_pk lzk_pk;
+int lzk_pk_save(const char* path, const lzk_groth16_pk* pk, const lzk_pk_info* info);
+int lzk_pk_load(const char* path, lzk_pk** out, lzk_groth16_pk* view, lzk_pk_info* info);
+int lzk_pk_free(lzk_pk* pk);
+
 /* Proof wire format (LZK_PROOF_WIRE_BYTES): the affine coordinates of A, B
  * and C as canonical (not Montgomery) little-endian 256-bit integers, in the
  * order A.x, A.y, B.x.c0, B.x.c1, B.y.c0, B.y.c1, C.x, C.y; a point at
@@ -406,6 +436,13 @@ int lzk_msm_set_window(int group, uint32_t log_n, uint32_t window_bits);
  * Replaces the reference's synchronising Timer/CUDA_DEBUG pairs
  * (timer.cu:3-16, device-utils.cuh:3). */
 void lzk_trace_enable(int on);
+/* NVTX ranges for the same named regions (independent of
+ * lzk_trace_enable): each region's host-side enqueue -- the calls that
+ * launch its kernels -- becomes one NVTX range (nvtxRangeStartA/End, so
+ * regions on different streams may overlap), which a profiler such as
+ * Nsight Systems shows beside the kernels they launched.  Off by default;
+ * without a profiler attached a range costs a few nanoseconds. */
+void lzk_trace_nvtx(int on);
 /* Restrict tracing to the comma-separated region names (NULL or "" = all
  * regions).  Every traced region records two timing events in its stream,
  * which costs a few microseconds of stream ordering each (about 1 % of a
@@ -427,6 +464,11 @@ typedef struct lzk_trace_span {
     double end_ms;
 } lzk_trace_span;
 int lzk_trace_timeline(lzk_trace_span* spans, size_t cap, size_t* count);
+/* Testing hook: after `after` more device allocations, every allocation
+ * the library makes fails as if the device were out of memory (LZK_ENOMEM
+ * from the call that needed it, with everything it had allocated released);
+ * a negative value turns the failures off.  Process-wide. */
+int lzk_debug_fail_allocations(long long after);
 /* Number of kernels this library has launched so far (all devices). */
 uint64_t lzk_launch_count(void);
 /* Measured 32-bit integer multiply-add rate of the current device

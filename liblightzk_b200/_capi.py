@@ -47,6 +47,9 @@ SIGNATURES = {
     "lzk_prover_device_bytes": (c_sz, [c_p]),
     "lzk_groth16_prove": (c_i, [c_p, c_p, c_p, c_p, c_p, c_p]),
     "lzk_groth16_proof_to_wire": (c_i, [c_p, c_p, c_p]),
+    "lzk_pk_save": (c_i, [ctypes.c_char_p, c_p, c_p]),
+    "lzk_pk_load": (c_i, [ctypes.c_char_p, c_p, c_p, c_p]),
+    "lzk_pk_free": (c_i, [c_p]),
     "lzk_groth16_proof_from_wire": (c_i, [c_p, c_p, c_p, c_p]),
     "lzk_server_create": (c_i, [c_p, c_p]),
     "lzk_server_add_circuit": (c_i, [c_p, c_p, c_p]),
@@ -63,6 +66,7 @@ SIGNATURES = {
     "lzk_batch_plan_destroy": (c_i, [c_p]),
     "lzk_msm_set_window": (c_i, [c_i, c_u32, c_u32]),
     "lzk_trace_enable": (None, [c_i]),
+    "lzk_trace_nvtx": (None, [c_i]),
     "lzk_trace_reset": (None, []),
     "lzk_trace_only": (c_i, [ctypes.c_char_p]),
     "lzk_trace_get": (c_i, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_uint64)]),
@@ -70,6 +74,7 @@ SIGNATURES = {
     "lzk_probe_imad_rate": (c_i, [ctypes.POINTER(ctypes.c_double)]),
     "lzk_probe_mont_rate": (c_i, [ctypes.POINTER(ctypes.c_double)]),
     "lzk_launch_count": (ctypes.c_uint64, []),
+    "lzk_debug_fail_allocations": (c_i, [ctypes.c_longlong]),
 }
 
 

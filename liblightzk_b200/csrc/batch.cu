@@ -254,7 +254,7 @@ static int create_plan(const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_des
     size_t o_la0 = cv.take<X>(std::max<uint64_t>(p->lvl, 1)), o_la1 = cv.take<X>(std::max<uint64_t>(p->lvl, 1));
     size_t o_wres = cv.take<X>(std::max<uint64_t>(p->total_windows, 1));
     p->ws_bytes = cv.off;
-    if (cudaMalloc(&p->ws, p->ws_bytes) != cudaSuccess) { cudaGetLastError(); return LZK_ENOMEM; }
+    LZK_TRY(dev_malloc(reinterpret_cast<void**>(&p->ws), p->ws_bytes));
     char* b = p->ws;
     p->d_desc = reinterpret_cast<BDesc*>(b + o_desc);
     p->d_ptsoff = reinterpret_cast<uint64_t*>(b + o_ptsoff);
@@ -286,7 +286,7 @@ static int create_plan(const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_des
         for (size_t s0 = 0; s0 < kv.second.size(); s0 += 65535) {
             size_t cnt = std::min<size_t>(65535, kv.second.size() - s0);
             lzk_batch_plan::NGroup g{kv.first.first, kv.first.second, (uint32_t)cnt, nullptr};
-            if (cudaMalloc(&g.ptrs, sizeof(Fr*) * cnt) != cudaSuccess) { cudaGetLastError(); return LZK_ENOMEM; }
+            LZK_TRY(dev_malloc(reinterpret_cast<void**>(&g.ptrs), sizeof(Fr*) * cnt));
             p->ngroups.push_back(g);
             LZK_CUDA(cudaMemcpy(g.ptrs, kv.second.data() + s0, sizeof(Fr*) * cnt, cudaMemcpyHostToDevice));
         }

@@ -22,6 +22,43 @@ void keep_pool_cached()
     done[dev] = true;
 }
 
+// remaining allocations before the forced failures begin; -1 = none forced
+static std::atomic<long long> g_fail_after{-1};
+
+static bool alloc_forced_to_fail()
+{
+    long long v = g_fail_after.load();
+    while (v >= 0) {
+        if (v == 0) return true;
+        if (g_fail_after.compare_exchange_weak(v, v - 1)) return false;
+    }
+    return false;
+}
+
+int dev_malloc(void** p, size_t bytes)
+{
+    *p = nullptr;
+    if (alloc_forced_to_fail()) return LZK_ENOMEM;
+    if (cudaMalloc(p, bytes ? bytes : 16) != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return LZK_ENOMEM;
+    }
+    return LZK_OK;
+}
+
+int dev_malloc_async(void** p, size_t bytes, cudaStream_t st)
+{
+    *p = nullptr;
+    if (alloc_forced_to_fail()) return LZK_ENOMEM;
+    if (cudaMallocAsync(p, bytes ? bytes : 16, st) != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return LZK_ENOMEM;
+    }
+    return LZK_OK;
+}
+
 unsigned sm_count()
 {
     static std::atomic<unsigned> cached[64];
@@ -54,8 +91,15 @@ const char* lzk_status_string(int status)
         case LZK_EBUSY: return "busy (pending, or refused by the memory budget)";
         case LZK_ECANCELED: return "request cancelled";
         case LZK_EREJECTED: return "request can never fit the memory budget";
+        case LZK_EIO: return "file cannot be read or written, or is not a valid key file";
         default: return "unknown status";
     }
+}
+
+int lzk_debug_fail_allocations(long long after)
+{
+    lzk::g_fail_after.store(after < 0 ? -1 : after);
+    return LZK_OK;
 }
 
 const char* lzk_version(void) { return "liblzk_b200 0.1 (sm_100a)"; }

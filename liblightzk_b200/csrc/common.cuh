@@ -49,6 +49,13 @@ void trace_end(void* h, cudaStream_t st);
 // stream-ordered scratch of repeated calls is served from the pool.
 void keep_pool_cached();
 
+// Every device allocation of the library goes through these two: cudaMalloc
+// and stream-ordered cudaMallocAsync, LZK_OK or LZK_ENOMEM (the CUDA error
+// cleared).  lzk_debug_fail_allocations makes them fail on demand, so the
+// clean-up of every create path can be tested without running out of memory.
+int dev_malloc(void** p, size_t bytes);
+int dev_malloc_async(void** p, size_t bytes, cudaStream_t st);
+
 // Streaming multiprocessors of the current device (queried once per device
 // and cached); grid-stride kernels size their grids in multiples of it.
 unsigned sm_count();
@@ -72,8 +79,7 @@ struct Scratch {
         }
         if (need == 0) return LZK_OK;
         keep_pool_cached();
-        cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&base), need, stream);
-        if (e != cudaSuccess) { cudaGetLastError(); base = nullptr; return LZK_ENOMEM; }
+        if (dev_malloc_async(reinterpret_cast<void**>(&base), need, stream) != LZK_OK) { base = nullptr; return LZK_ENOMEM; }
         owned = true;
         return LZK_OK;
     }

@@ -19,7 +19,11 @@
 //     coefficients M+1 .. 2M-1.
 //   LZK_PROVE_STANDARD is the standard quotient on the coset g<w_M>:
 //     iNTT_M, coset NTT_M, (A*B - C) * (g^M - 1)^-1, coset iNTT_M,
-//     H scalars = h_0 .. h_{M-2}; all transforms stay at size M.
+//     H scalars = h_0 .. h_{M-2}; all transforms stay at size M and none
+//     has a bit-reversal pass: decimation-in-frequency passes for the
+//     inverses and decimation-in-time passes for the coset transforms, so
+//     the H coefficients end in bit-reversed order, the order in which the
+//     prover stores the H query.
 // Phase 6 (groth16.cuh:211-215) runs on the device.  The reference forms
 //   Ar = a1 + A + r d1,  Bs1 = b1 + B1 + s d1,  Bs2 = b2 + B2 + s d2,
 //   Krs = s Ar + r Bs1 + (-r s) d1 + L,  proof = (Ar, Bs2, Krs + H);
@@ -135,6 +139,16 @@ __global__ void k_abc(Fr* __restrict__ x0, const Fr* __restrict__ x1, const Fr* 
     }
 }
 
+// out[i] = in[brev(i)] over log_m-bit indices, i < n (n <= 2^log_m - 1, so
+// brev(i) < n: the bit reversal is an involution that fixes 2^log_m - 1)
+__global__ void k_gather_brev(const Aff<Fq>* __restrict__ in, size_t n, uint32_t log_m, Aff<Fq>* __restrict__ out)
+{
+    for (uint64_t i = gtid(); i < n; i += gstride()) {
+        size_t j = (size_t)(__brevll((unsigned long long)i) >> (64 - log_m));
+        st_elem(out + i, ldg_elem(in + j));
+    }
+}
+
 // (g^M - 1)^-1, g = 5
 __global__ void k_zinv(uint32_t log_m, Fr* out)
 {
@@ -155,7 +169,7 @@ template <class T>
 static int dalloc(size_t* acct, T** ptr, size_t count)
 {
     size_t b = count * sizeof(T);
-    if (cudaMalloc(reinterpret_cast<void**>(ptr), b ? b : 16) != cudaSuccess) { cudaGetLastError(); return LZK_ENOMEM; }
+    LZK_TRY(dev_malloc(reinterpret_cast<void**>(ptr), b));
     *acct += b;
     return LZK_OK;
 }
@@ -279,8 +293,27 @@ static int create(const lzk_groth16_circuit* c, const lzk_groth16_pk* pk, int mo
     if (p->nl)
         LZK_TRY(lzk_g1_precompute(pk->l_query, p->nl, p->c, p->wins, reinterpret_cast<lzk_g1_affine_t*>(p->tab[2]),
                                   p->tn[2], st));
-    LZK_TRY(lzk_g1_precompute(pk->h_query, p->M - 1, p->c, p->wins,
-                              reinterpret_cast<lzk_g1_affine_t*>(p->tab[2] + p->nl), p->tn[2], st));
+    {
+        // standard mode leaves the H coefficients in bit-reversed order (the
+        // transforms skip their bit reversal), so its H table holds the
+        // query in that order: entry i = h_query[brev(i)]
+        const lzk_g1_affine_t* hq = pk->h_query;
+        Aff<Fq>* perm = nullptr;
+        if (mode == LZK_PROVE_STANDARD) {
+            size_t scratch = 0;
+            LZK_TRY(dalloc(&scratch, &perm, p->M - 1));
+            k_gather_brev<<<grid_for(p->M - 1, 256, sm_count() * 8), 256, 0, st>>>(
+                reinterpret_cast<const Aff<Fq>*>(pk->h_query), p->M - 1, p->log_m, perm); note_launch();
+            hq = reinterpret_cast<const lzk_g1_affine_t*>(perm);
+        }
+        int rc = lzk_g1_precompute(hq, p->M - 1, p->c, p->wins, reinterpret_cast<lzk_g1_affine_t*>(p->tab[2] + p->nl),
+                                   p->tn[2], st);
+        if (perm) {
+            cudaStreamSynchronize(st);
+            cudaFree(perm);
+        }
+        LZK_TRY(rc);
+    }
     p->tn2 = c->n_vars;
     LZK_TRY(dalloc(&p->bytes, &p->tab2, (size_t)p->wins * p->tn2));
     LZK_TRY(lzk_g2_precompute(pk->b2_query, p->tn2, p->c, p->wins, reinterpret_cast<lzk_g2_affine_t*>(p->tab2), p->tn2, st));
@@ -401,10 +434,18 @@ int prove_ctx(const lzk_prover* p, ProveCtx* x, const Fr* z, const lzk_fr_t* r, 
         LZK_TRY(ntt_run(x0, p->log_m + 1, LZK_NTT_INVERSE, 1, 0, t4.consts + 2, st));
         hs = x0 + p->M + 1;
     } else {
-        LZK_TRY(ntt_run(x->x, p->log_m, LZK_NTT_INVERSE, 3, p->L, nullptr, st));
-        LZK_TRY(ntt_run(x->x, p->log_m, LZK_NTT_COSET_FORWARD, 3, p->L, nullptr, st));
+        // no bit reversal anywhere: the inverse transforms are DIF passes
+        // (natural -> bit-reversed, unscaled), the coset transforms DIT passes
+        // (bit-reversed -> natural) whose first pass applies M^-1 g^j to
+        // coefficient j, and the last inverse's final pass applies
+        // M^-1 g^-j, leaving h_j at position brev(j) (the H table's order)
+        NttTables t; CosetTables ct;
+        LZK_TRY(get_tables(p->log_m, t, ct));
+        const Fr* minv = t.consts + 2;
+        LZK_TRY(ntt_passes(x->x, p->log_m, 3, p->L, t.tw[1], false, NttEdge{}, NttEdge{}, st));
+        LZK_TRY(ntt_passes(x->x, p->log_m, 3, p->L, t.tw[0], true, NttEdge{ct.lo[0], ct.hi[0], minv, 1}, NttEdge{}, st));
         k_abc<<<grid_for(p->L, 256, sm_count() * 8), 256, 0, st>>>(x0, x1, x2, p->L, p->zinv); note_launch();
-        LZK_TRY(ntt_run(x0, p->log_m, LZK_NTT_COSET_INVERSE, 1, 0, nullptr, st));
+        LZK_TRY(ntt_passes(x0, p->log_m, 1, 0, t.tw[1], false, NttEdge{}, NttEdge{ct.lo[1], ct.hi[1], minv, 1}, st));
         hs = x0;
     }
     trace_end(tr_h, st);

@@ -173,9 +173,10 @@ static int comb_table(const Aff<F>** out, int group)
     auto it = g_comb[group].find(dev);
     if (it != g_comb[group].end()) { *out = static_cast<const Aff<F>*>(it->second); return LZK_OK; }
     Aff<F>* T = nullptr;
-    if (cudaMalloc(&T, 32 * 256 * sizeof(Aff<F>)) != cudaSuccess) { cudaGetLastError(); return LZK_ENOMEM; }
+    LZK_TRY(dev_malloc(reinterpret_cast<void**>(&T), 32 * 256 * sizeof(Aff<F>)));
     cudaStream_t st;
-    LZK_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    cudaError_t se = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (se != cudaSuccess) { cudaFree(T); return cuda_status(se); }
     int rc = comb_build<F>(nullptr, T, st);
     if (rc == LZK_OK) rc = cuda_status(cudaStreamSynchronize(st));
     cudaStreamDestroy(st);

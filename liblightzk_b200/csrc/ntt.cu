@@ -25,8 +25,6 @@ constexpr uint32_t kNttElems = 2048;   // elements per block in a pass (64 KB sm
 constexpr uint32_t kNttThreads = 256;
 constexpr uint32_t kPowLoBits = 12;    // g^j = lo[j & 4095] * hi[j >> 12]
 
-enum : uint32_t { NTT_PRE_COSET = 1u };
-
 // Montgomery form of w_28 = 5^((r-1)/2^28) and of g = 5
 __device__ __forceinline__ Fr root28()
 {
@@ -99,9 +97,12 @@ int get_tables(uint32_t k, NttTables& out, CosetTables& cos)
     if (it == g_ntt_tables.end()) {
         NttTables t;
         size_t half = k ? (size_t(1) << (k - 1)) : 1;
-        if (cudaMalloc(&t.consts, 8 * sizeof(Fr)) != cudaSuccess || cudaMalloc(&t.tw[0], half * sizeof(Fr)) != cudaSuccess ||
-            cudaMalloc(&t.tw[1], half * sizeof(Fr)) != cudaSuccess) {
-            cudaGetLastError();
+        if (dev_malloc(reinterpret_cast<void**>(&t.consts), 8 * sizeof(Fr)) != LZK_OK ||
+            dev_malloc(reinterpret_cast<void**>(&t.tw[0]), half * sizeof(Fr)) != LZK_OK ||
+            dev_malloc(reinterpret_cast<void**>(&t.tw[1]), half * sizeof(Fr)) != LZK_OK) {
+            cudaFree(t.consts);
+            cudaFree(t.tw[0]);
+            cudaFree(t.tw[1]);
             rc = LZK_ENOMEM;
         } else {
             k_ntt_consts<<<1, 32, 0, st>>>(k, t.consts); note_launch();
@@ -117,8 +118,12 @@ int get_tables(uint32_t k, NttTables& out, CosetTables& cos)
         Fr* cst = g_ntt_tables[{dev, k}].consts;
         bool ok = true;
         for (int d = 0; d < 2 && ok; d++)
-            ok = cudaMalloc(&c.lo[d], nlo * sizeof(Fr)) == cudaSuccess && cudaMalloc(&c.hi[d], nhi * sizeof(Fr)) == cudaSuccess;
-        if (!ok) { cudaGetLastError(); rc = LZK_ENOMEM; }
+            ok = dev_malloc(reinterpret_cast<void**>(&c.lo[d]), nlo * sizeof(Fr)) == LZK_OK &&
+                 dev_malloc(reinterpret_cast<void**>(&c.hi[d]), nhi * sizeof(Fr)) == LZK_OK;
+        if (!ok) {
+            for (int d = 0; d < 2; d++) { cudaFree(c.lo[d]); cudaFree(c.hi[d]); }
+            rc = LZK_ENOMEM;
+        }
         else {
             for (int d = 0; d < 2; d++) {
                 k_powers<<<grid_for(nlo / 64, 128), 128, 0, st>>>(cst + 3 + d, c.lo[d], nlo); note_launch();
@@ -144,12 +149,36 @@ __device__ __forceinline__ Fr coset_pow(const Fr* lo, const Fr* hi, size_t j)
     return mul(ldg_elem(lo + (j & ((1u << kPowLoBits) - 1))), ldg_elem(hi + (j >> kPowLoBits)));
 }
 
-// m DIF stages s0..s0+m-1 over groups of 2^m elements that differ in index
-// bits [lowbits, lowbits+m); R groups with consecutive (outer, low) index
-// per block.  `batch` transforms of size 2^k lie `bstride` elements apart.
+__device__ __forceinline__ size_t brev_k(size_t j, uint32_t k)
+{
+    return k ? (size_t)(__brevll((unsigned long long)j) >> (64 - k)) : 0;
+}
+
+// Factor a pass applies to each element as it loads it (the first pass) or
+// stores it (the last pass): x * scale * g^e, e = the position j, or, with
+// brev set, the coefficient index brev(j) that a bit-reversed position
+// holds; a null scale or null power tables stand for 1.
+__device__ __forceinline__ Fr edge_apply(const NttEdge& ed, const Fr& sc, Fr x, size_t j, uint32_t k)
+{
+    if (ed.scale) x = mul(x, sc);
+    if (ed.lo) x = mul(x, coset_pow(ed.lo, ed.hi, ed.brev ? brev_k(j, k) : j));
+    return x;
+}
+
+// m radix-2 stages in shared memory over groups of 2^m elements that differ
+// in index bits [lowbits, lowbits+m); R groups with consecutive (outer, low)
+// index per block.  `batch` transforms of size 2^k lie `bstride` elements
+// apart (or at ptrs[blockIdx.y]).
+//   DIF (decimation in frequency): stages s0 .. s0+m-1, natural order in,
+//     bit-reversed out after all passes; c[j] = lo + hi, c[j^h] =
+//     (lo - hi) w^((j mod h) << s) (poly.cuh:38-39).
+//   DIT (decimation in time): stages t = lowbits .. lowbits+m-1, bit-reversed
+//     order in, natural out; with u = w^((j mod 2^t) << (k-1-t)) hi,
+//     c[j] = lo + u, c[j + 2^t] = lo - u.
+// Both compute X_k = sum_j a_j w^(jk).
+template <bool DIT>
 __global__ void __launch_bounds__(kNttThreads) k_ntt_pass(Fr* __restrict__ data, NttPass p, const Fr* __restrict__ tw,
-                                                           uint32_t flags, const Fr* __restrict__ clo,
-                                                           const Fr* __restrict__ chi, size_t bstride,
+                                                           NttEdge pre, NttEdge post, size_t bstride,
                                                            Fr* const* __restrict__ ptrs)
 {
     extern __shared__ uint4 smem_raw[];
@@ -159,41 +188,47 @@ __global__ void __launch_bounds__(kNttThreads) k_ntt_pass(Fr* __restrict__ data,
     const uint32_t rbits = __ffs(R) - 1;
     const size_t lowmask = (size_t(1) << p.lowbits) - 1;
     const uint32_t tot = G * R;
+    const bool use_pre = pre.scale || pre.lo, use_post = post.scale || post.lo;
+    const Fr psc = pre.scale ? ldg_elem(pre.scale) : Fr::one();
+    const Fr qsc = post.scale ? ldg_elem(post.scale) : Fr::one();
     for (uint32_t i = threadIdx.x; i < tot; i += blockDim.x) {
         uint32_t g = i >> rbits, r = i & (R - 1);
         size_t cidx = (size_t)blockIdx.x * R + r;
-        size_t j = ((cidx >> p.lowbits) << (p.k - p.s0)) | ((size_t)g << p.lowbits) | (cidx & lowmask);
+        size_t j = ((cidx >> p.lowbits) << (p.lowbits + p.m)) | ((size_t)g << p.lowbits) | (cidx & lowmask);
         Fr x = ldg_elem(d + j);
-        if (flags & NTT_PRE_COSET) x = mul(x, coset_pow(clo, chi, j));
+        if (use_pre) x = edge_apply(pre, psc, x, j, p.k);
         st_elem(sm + i, x);
     }
     __syncthreads();
     for (uint32_t t = 0; t < p.m; t++) {
-        uint32_t hb = p.m - 1 - t;        // half = 2^hb groups
-        uint32_t s = p.s0 + t;
+        // DIF: group-index bit hb = m-1-t; DIT: bit hb = t
+        uint32_t hb = DIT ? t : p.m - 1 - t;
         for (uint32_t b = threadIdx.x; b < tot / 2; b += blockDim.x) {
             uint32_t r = b & (R - 1), gb = b >> rbits;
             uint32_t g = ((gb >> hb) << (hb + 1)) | (gb & ((1u << hb) - 1));
             uint32_t i0 = (g << rbits) | r, i1 = ((g + (1u << hb)) << rbits) | r;
             size_t low = ((size_t)blockIdx.x * R + r) & lowmask;
-            size_t e = ((((size_t)(g & ((1u << hb) - 1))) << p.lowbits) | low) << s;
+            size_t jm = (((size_t)(g & ((1u << hb) - 1))) << p.lowbits) | low;
             Fr lo = ld_elem(sm + i0), hi = ld_elem(sm + i1);
-            st_elem(sm + i0, add(lo, hi));
-            st_elem(sm + i1, mul(sub(lo, hi), ldg_elem(tw + e)));
+            if (DIT) {
+                Fr u = mul(hi, ldg_elem(tw + (jm << (p.k - 1 - (p.lowbits + t)))));
+                st_elem(sm + i0, add(lo, u));
+                st_elem(sm + i1, sub(lo, u));
+            } else {
+                st_elem(sm + i0, add(lo, hi));
+                st_elem(sm + i1, mul(sub(lo, hi), ldg_elem(tw + (jm << (p.s0 + t)))));
+            }
         }
         __syncthreads();
     }
     for (uint32_t i = threadIdx.x; i < tot; i += blockDim.x) {
         uint32_t g = i >> rbits, r = i & (R - 1);
         size_t cidx = (size_t)blockIdx.x * R + r;
-        size_t j = ((cidx >> p.lowbits) << (p.k - p.s0)) | ((size_t)g << p.lowbits) | (cidx & lowmask);
-        st_elem(d + j, ld_elem(sm + i));
+        size_t j = ((cidx >> p.lowbits) << (p.lowbits + p.m)) | ((size_t)g << p.lowbits) | (cidx & lowmask);
+        Fr x = ld_elem(sm + i);
+        if (use_post) x = edge_apply(post, qsc, x, j, p.k);
+        st_elem(d + j, x);
     }
-}
-
-__device__ __forceinline__ size_t brev_k(size_t j, uint32_t k)
-{
-    return (size_t)(__brevll((unsigned long long)j) >> (64 - k));
 }
 
 // In-place bit reversal; each output position pos is then multiplied by
@@ -206,7 +241,7 @@ __global__ void k_ntt_bitrev(Fr* __restrict__ data, uint32_t k, const Fr* __rest
     size_t n = size_t(1) << k;
     Fr sc = scale ? ldg_elem(scale) : Fr::one();
     for (uint64_t j = gtid(); j < n; j += gstride()) {
-        size_t r = k ? brev_k(j, k) : 0;
+        size_t r = brev_k(j, k);
         if (j > r) continue;
         Fr a = ld_elem(d + j), b = ld_elem(d + r);
         // after the swap position j holds b and position r holds a
@@ -225,34 +260,29 @@ int ntt_prepare_launch()
     LZK_CUDA(cudaGetDevice(&dev));
     std::lock_guard<std::mutex> g(mu);
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-        LZK_CUDA(cudaFuncSetAttribute(k_ntt_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttElems * sizeof(Fr)));
+        LZK_CUDA(cudaFuncSetAttribute(k_ntt_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttElems * sizeof(Fr)));
+        LZK_CUDA(cudaFuncSetAttribute(k_ntt_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttElems * sizeof(Fr)));
         attr_set[dev] = true;
     }
     return LZK_OK;
 }
 
-// Enqueue the passes of `count` transforms of size 2^k (natural order in,
-// natural order out) with twiddle table tw (w^e, e < n/2).
-static int ntt_enqueue(Fr* data, uint32_t k, uint32_t count, size_t bstride, const Fr* tw, const Fr* scale,
-                       const Fr* pre_lo, const Fr* pre_hi, const Fr* post_lo, const Fr* post_hi, cudaStream_t st,
-                       Fr* const* ptrs = nullptr)
+int ntt_passes(Fr* data, uint32_t k, uint32_t count, size_t bstride, const Fr* tw, bool dit, NttEdge pre,
+               NttEdge post, cudaStream_t st, Fr* const* ptrs)
 {
+    if (k == 0 || k > 30 || count == 0 || count > 65535 || (!data && !ptrs) || !tw) return LZK_EINVAL;
     LZK_TRY(ntt_prepare_launch());
-    if (k == 0) {
-        if (scale || post_lo || pre_lo) {
-            k_ntt_bitrev<<<dim3(1, count), 32, 0, st>>>(data, 0, scale, post_lo, post_hi, bstride, ptrs); note_launch();
-            return launch_status();
-        }
-        return LZK_OK;
-    }
-    uint32_t maxm = 11;
-    uint32_t P = (k + maxm - 1) / maxm;
-    size_t n = size_t(1) << k;
-    uint32_t s0 = 0;
+    const uint32_t maxm = 11;
+    const uint32_t P = (k + maxm - 1) / maxm;
+    const size_t n = size_t(1) << k;
+    uint32_t done = 0;   // stages done by earlier passes
     for (uint32_t q = 0; q < P; q++) {
-        uint32_t m = (k - s0) / (P - q);      // balanced split, larger passes last
+        uint32_t m = (k - done) / (P - q);    // balanced split, larger passes last
         NttPass pp;
-        pp.k = k; pp.s0 = s0; pp.m = m; pp.lowbits = k - s0 - m;
+        pp.k = k; pp.m = m;
+        // DIF passes take the top index bits first, DIT passes the bottom ones
+        pp.lowbits = dit ? done : k - done - m;
+        pp.s0 = dit ? 0 : done;
         uint32_t G = 1u << m;
         uint32_t R = kNttElems / G;
         if ((size_t)R > (n >> m)) R = (uint32_t)(n >> m);
@@ -260,10 +290,32 @@ static int ntt_enqueue(Fr* data, uint32_t k, uint32_t count, size_t bstride, con
         pp.R = R;
         size_t blocks = (n >> m) / R;
         size_t smem = (size_t)G * R * sizeof(Fr);
-        uint32_t flags = (q == 0 && pre_lo) ? NTT_PRE_COSET : 0u;
-        k_ntt_pass<<<dim3((unsigned)blocks, count), kNttThreads, smem, st>>>(data, pp, tw, flags, pre_lo, pre_hi, bstride, ptrs); note_launch();
-        s0 += m;
+        NttEdge a = q == 0 ? pre : NttEdge{}, b = q == P - 1 ? post : NttEdge{};
+        if (dit)
+            k_ntt_pass<true><<<dim3((unsigned)blocks, count), kNttThreads, smem, st>>>(data, pp, tw, a, b, bstride, ptrs);
+        else
+            k_ntt_pass<false><<<dim3((unsigned)blocks, count), kNttThreads, smem, st>>>(data, pp, tw, a, b, bstride, ptrs);
+        note_launch();
+        done += m;
     }
+    return launch_status();
+}
+
+// Enqueue `count` transforms of size 2^k (natural order in, natural order
+// out) with twiddle table tw (w^e, e < n/2): DIF passes, then the bit
+// reversal with the output factors.
+static int ntt_enqueue(Fr* data, uint32_t k, uint32_t count, size_t bstride, const Fr* tw, const Fr* scale,
+                       const Fr* pre_lo, const Fr* pre_hi, const Fr* post_lo, const Fr* post_hi, cudaStream_t st,
+                       Fr* const* ptrs = nullptr)
+{
+    LZK_TRY(ntt_prepare_launch());
+    if (k > 0) {
+        NttEdge pre{pre_lo, pre_hi, nullptr, 0};
+        LZK_TRY(ntt_passes(data, k, count, bstride, tw, false, pre, NttEdge{}, st, ptrs));
+    } else if (!(scale || post_lo || pre_lo)) {
+        return LZK_OK;
+    }
+    size_t n = size_t(1) << k;
     k_ntt_bitrev<<<dim3(grid_for(n, 256, sm_count() * 8), count), 256, 0, st>>>(data, k, scale, post_lo, post_hi, bstride, ptrs); note_launch();
     return launch_status();
 }

@@ -15,6 +15,19 @@ struct CosetTables {
     Fr* hi[2] = {nullptr, nullptr};  // g^(4096 i), g^-(4096 i) for i < 2^(26-12)
 };
 
+// Factor applied to every element as the first pass of a transform loads
+// it (pre) or the last pass stores it (post): x * scale * g^e with g^e from
+// the power tables lo/hi (g^j = lo[j & 4095] * hi[j >> 12]) and e the
+// element's position, or the bit reversal of its position when brev is set
+// (the coefficient index a bit-reversed position holds).  Null scale / null
+// tables: factor 1.
+struct NttEdge {
+    const Fr* lo = nullptr;
+    const Fr* hi = nullptr;
+    const Fr* scale = nullptr;
+    uint32_t brev = 0;
+};
+
 // cached per-device tables for size 2^k (built synchronously on first use)
 int get_tables(uint32_t k, NttTables& out, CosetTables& cos);
 // count transforms of size 2^k, `bstride` apart (or at ptrs[t], a device
@@ -25,5 +38,11 @@ int get_tables(uint32_t k, NttTables& out, CosetTables& cos);
 int ntt_prepare_launch();
 int ntt_run(Fr* data, uint32_t k, int dir, uint32_t count, size_t bstride, const Fr* scale_override, cudaStream_t st,
             Fr* const* ptrs = nullptr);
+// The passes of `count` transforms of size 2^k (k >= 1) with twiddle table
+// tw (w^e, e < n/2) and no bit reversal: DIF takes natural order to
+// bit-reversed order, DIT bit-reversed order to natural order.  pre applies
+// to the first pass's loads, post to the last pass's stores.
+int ntt_passes(Fr* data, uint32_t k, uint32_t count, size_t bstride, const Fr* tw, bool dit, NttEdge pre,
+               NttEdge post, cudaStream_t st, Fr* const* ptrs = nullptr);
 
 }  // namespace lzk

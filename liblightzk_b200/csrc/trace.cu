@@ -7,6 +7,7 @@
 // and durations are resolved when the host asks for them.
 #include "common.cuh"
 #include "field.cuh"
+#include <nvtx3/nvToolsExt.h>
 #include <atomic>
 #include <map>
 #include <mutex>
@@ -18,6 +19,8 @@ namespace lzk {
 struct TraceRec {
     std::string name;
     cudaEvent_t a, b;
+    nvtxRangeId_t nvtx = 0;   // NVTX range of the region's enqueue, 0 = none
+    bool events = false;      // timing events recorded
 };
 
 struct TraceSpan {
@@ -39,6 +42,7 @@ static std::vector<TraceSpan> g_tr_spans;
 constexpr size_t kMaxSpans = 1u << 16;
 
 static std::atomic<unsigned long long> g_launches{0};
+static std::atomic<bool> g_nvtx{false};
 
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
@@ -46,23 +50,28 @@ bool trace_on() { return g_tr_on; }
 
 void* trace_begin(const char* name, cudaStream_t st)
 {
-    if (!g_tr_on) return nullptr;
-    {
+    bool ev = g_tr_on, nv = g_nvtx.load(std::memory_order_relaxed);
+    if (!ev && !nv) return nullptr;
+    if (ev) {
         std::lock_guard<std::mutex> g(g_tr_mu);
         if (!g_tr_only.empty()) {
             bool hit = false;
             for (const auto& n : g_tr_only) hit = hit || n == name;
-            if (!hit) return nullptr;
+            ev = hit;
         }
     }
-    TraceRec* r = new TraceRec{name, nullptr, nullptr};
-    cudaEventCreate(&r->a);
-    cudaEventCreate(&r->b);
-    {
-        std::lock_guard<std::mutex> g(g_tr_mu);
-        if (!g_tr_origin && cudaEventCreate(&g_tr_origin) == cudaSuccess) cudaEventRecord(g_tr_origin, st);
+    if (!ev && !nv) return nullptr;
+    TraceRec* r = new TraceRec{name, nullptr, nullptr, 0, ev};
+    if (nv) r->nvtx = nvtxRangeStartA(name);
+    if (ev) {
+        cudaEventCreate(&r->a);
+        cudaEventCreate(&r->b);
+        {
+            std::lock_guard<std::mutex> g(g_tr_mu);
+            if (!g_tr_origin && cudaEventCreate(&g_tr_origin) == cudaSuccess) cudaEventRecord(g_tr_origin, st);
+        }
+        cudaEventRecord(r->a, st);
     }
-    cudaEventRecord(r->a, st);
     return r;
 }
 
@@ -70,9 +79,12 @@ void trace_end(void* h, cudaStream_t st)
 {
     if (!h) return;
     TraceRec* r = static_cast<TraceRec*>(h);
-    cudaEventRecord(r->b, st);
-    std::lock_guard<std::mutex> g(g_tr_mu);
-    g_tr_pending.push_back(*r);
+    if (r->nvtx) nvtxRangeEnd(r->nvtx);
+    if (r->events) {
+        cudaEventRecord(r->b, st);
+        std::lock_guard<std::mutex> g(g_tr_mu);
+        g_tr_pending.push_back(*r);
+    }
     delete r;
 }
 
@@ -150,6 +162,8 @@ using namespace lzk;
 extern "C" {
 
 uint64_t lzk_launch_count(void) { return g_launches.load(); }
+
+void lzk_trace_nvtx(int on) { g_nvtx.store(on != 0); }
 
 void lzk_trace_enable(int on)
 {

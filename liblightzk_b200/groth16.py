@@ -42,6 +42,13 @@ class Pk(ctypes.Structure):
                 ("delta1", _G1Aff), ("beta2", _G2Aff), ("delta2", _G2Aff)]
 
 
+class PkInfo(ctypes.Structure):
+    """struct lzk_pk_info"""
+
+    _fields_ = [("n_vars", ctypes.c_uint64), ("n_public", ctypes.c_uint64), ("log_domain", ctypes.c_uint32),
+                ("version", ctypes.c_uint32)]
+
+
 def _fill(struct, t):
     """copy a device point tensor's limbs into a ctypes affine struct"""
     a = to_host(t).reshape(-1)
@@ -86,20 +93,64 @@ def from_wire(wire, stream=None):
     return proof, bad
 
 
+def pk_struct(pk):
+    """struct lzk_groth16_pk of a key: a LoadedKey's view, or one built from
+    the device tensors of a synth.ProvingKey"""
+    if isinstance(pk, LoadedKey):
+        return pk.view
+    k = Pk()
+    k.a_query, k.b1_query, k.b2_query = ptr(pk.a), ptr(pk.b1), ptr(pk.b2)
+    k.l_query, k.h_query = ptr(pk.l), ptr(pk.h)
+    _fill(k.alpha1, pk.alpha1)
+    _fill(k.beta1, pk.beta1)
+    _fill(k.delta1, pk.delta1)
+    _fill(k.beta2, pk.beta2)
+    _fill(k.delta2, pk.delta2)
+    return k
+
+
+def save_key(path, pk, circuit):
+    """write the proving key of `circuit` to a key file (lzk_pk_save)"""
+    info = PkInfo(circuit.n_vars, circuit.n_public, circuit.log_m, 0)
+    torch.cuda.synchronize()
+    _capi.call("lzk_pk_save", str(path).encode(), ctypes.byref(pk_struct(pk)), ctypes.byref(info))
+
+
+class LoadedKey:
+    """a key file loaded into device memory (lzk_pk_load); `view` is the
+    lzk_groth16_pk for lzk_prover_create, `info` the circuit shape"""
+
+    def __init__(self, path):
+        self.view, self.info = Pk(), PkInfo()
+        h = ctypes.c_void_p()
+        _capi.call("lzk_pk_load", str(path).encode(), ctypes.byref(h), ctypes.byref(self.view),
+                   ctypes.byref(self.info))
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            _capi.call("lzk_pk_free", self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Prover:
     def __init__(self, circuit, pk, mode=STANDARD, window_bits=0):
+        """pk: a synth.ProvingKey (device tensors) or a LoadedKey"""
         self.circuit = circuit   # keeps the CSR tensors alive
         c = Circuit()
         c.A, c.B, c.C = circuit.A.desc(), circuit.B.desc(), circuit.C.desc()
         c.n_vars, c.n_public, c.log_domain = circuit.n_vars, circuit.n_public, circuit.log_m
-        k = Pk()
-        k.a_query, k.b1_query, k.b2_query = ptr(pk.a), ptr(pk.b1), ptr(pk.b2)
-        k.l_query, k.h_query = ptr(pk.l), ptr(pk.h)
-        _fill(k.alpha1, pk.alpha1)
-        _fill(k.beta1, pk.beta1)
-        _fill(k.delta1, pk.delta1)
-        _fill(k.beta2, pk.beta2)
-        _fill(k.delta2, pk.delta2)
+        if isinstance(pk, LoadedKey):
+            i = pk.info
+            if (i.n_vars, i.n_public, i.log_domain) != (circuit.n_vars, circuit.n_public, circuit.log_m):
+                raise ValueError("key file was saved for another circuit shape")
+        k = pk_struct(pk)
         self._c, self._k = c, k
         h = ctypes.c_void_p()
         _capi.call("lzk_prover_create", ctypes.byref(c), ctypes.byref(k), mode, window_bits, ctypes.byref(h))

@@ -48,6 +48,17 @@ class Server:
         self.provers.append(prover)
         return cid.value
 
+    def add_key_file(self, circuit, path, mode=0, window_bits=0):
+        """make a resident prover for `circuit` from its key file (the loaded
+        key is freed once the prover has built its tables) and add it"""
+        from .groth16 import LoadedKey, Prover
+        key = LoadedKey(path)
+        try:
+            prover = Prover(circuit, key, mode=mode, window_bits=window_bits)
+        finally:
+            key.close()
+        return self.add(prover)
+
     def submit(self, cid, z, r, s, pinned=False):
         """z: numpy uint64 (n_vars, 4) or a pinned CPU torch tensor (pinned=True: it must
         stay unchanged until the request completes)"""

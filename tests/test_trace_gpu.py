@@ -70,3 +70,28 @@ def test_trace_only_filter(cuda):
     assert {t[0] for t in _capi.trace_timeline()} == {"msm_g1_accumulate", "groth16_assemble"}
     _capi.trace_reset()
     prover.close()
+
+
+def test_nvtx_ranges_beside_events(cuda, orc, rng_state):
+    """NVTX ranges on, alone and together with the event tracer: results and
+    event timings are unaffected (the ranges only mark host-side enqueues)"""
+    from helpers import bases, same_point, scalars
+    from liblightzk_b200 import _capi, device, msm
+    n = 3000
+    s, b = scalars(orc, n, rng_state), bases(orc, 1, n, rng_state)
+    want = orc.msm(1, s, b)
+    lib = _capi.lib()
+    try:
+        lib.lzk_trace_nvtx(1)
+        got = device.to_host(msm.msm(1, device.to_device(s), device.to_device(b)))
+        assert same_point(orc, 1, got, want)
+        _capi.trace_reset()
+        _capi.trace_enable(True)
+        got = device.to_host(msm.msm(1, device.to_device(s), device.to_device(b)))
+        _capi.trace_enable(False)
+        assert same_point(orc, 1, got, want)
+        ms, cnt = _capi.trace_get("msm_g1")
+        assert cnt == 1 and ms > 0
+    finally:
+        lib.lzk_trace_nvtx(0)
+        _capi.trace_enable(False)
