@@ -306,12 +306,21 @@ def run_batch_case(args):
 
     one_by_one()
     seq_ms = timed(one_by_one, args.reps)
+    # per-phase device times of one eager (uncaptured) run of the plan
+    from liblightzk_b200 import _capi
+    _capi.trace_reset()
+    _capi.trace_enable(True)
+    plan.run(use_graph=False, stream=stream)
+    torch.cuda.synchronize()
+    _capi.trace_enable(False)
+    phases = {ph: _capi.trace_get(f"batch_{ph}")[0] for ph in ("msm_sort", "msm_accumulate", "msm_fixup",
+                                                                "msm_reduce", "msm_finish", "ntt")}
     pts = sum(int(m[0].shape[0]) for m in msms)
     elems = sum(1 << k for _, k, _ in ntts)
     print(json.dumps({"case": "batch", "msms": len(msms), "ntts": len(ntts), "msm_points": pts,
                       "ntt_elements": elems, "plan_graph_ms": plan_ms, "one_by_one_ms": seq_ms,
                       "speedup": float(np.median(seq_ms) / np.median(plan_ms)),
-                      "plan_device_bytes": plan.device_bytes(),
+                      "plan_device_bytes": plan.device_bytes(), "phases_ms_eager": phases,
                       "tuned_windows": {lg: v[0] for lg, v in tuned.items()}}), flush=True)
 
 
@@ -704,16 +713,20 @@ def main():
     alg_imad = avg_pts * W * FP_MUL_PER_G1_MADD * IMAD_PER_FP_MUL
     acc_avg_ms = acc_ms / max(acc_n, 1)
     achieved = alg_imad / (acc_avg_ms * 1e-3) if acc_n else None
-    traffic = None
+    traffic = pipe_util = pipe_util_probe = None
     prof = os.path.join(ROOT, "profiles", "msm_g1_accumulate_traffic.json")
     if os.path.exists(prof):
         try:
             tj = json.load(open(prof))
             # per average launch of this proof, scaled by its points from the
             # captured launch (traffic grows with the entries)
-            traffic = tj["bytes_per_launch_at_2e20"] * avg_pts / tj.get("points_at_2e20", 1052674)
+            traffic = tj["bytes_per_launch_at_2e20"] * avg_pts / tj["points_at_2e20"]
+            # ncu's multiplier (fmaheavy) pipe activity of that launch, and of
+            # the product probe that sets `peak`
+            pipe_util = tj["fmaheavy_pipe_active_pct"] / 100.0
+            pipe_util_probe = tj["fmaheavy_pipe_active_pct_probe"] / 100.0
         except Exception:
-            traffic = None
+            traffic = pipe_util = pipe_util_probe = None
 
     iso_line = None
     if iso_n:
@@ -766,6 +779,9 @@ def main():
                      "peak_source": "measured: lzk_probe_mont_rate (independent Fq Montgomery products in the "
                                     "kernels' instruction form, full occupancy) x 264 IMAD-class per product",
                      "mont_products_per_s": mont_rate,
+                     "pipe_util": pipe_util, "pipe_util_probe": pipe_util_probe,
+                     "pipe_util_source": "ncu sm__pipe_fmaheavy_cycles_active of one G1 accumulation launch at 2^20 "
+                                         "and of the probe (profiles/k_accumulate_2e20.md)",
                      "peak_mad_chains_T": mad_chain_rate / 1e12,
                      "algorithmic_imad_per_launch": alg_imad, "avg_launch_ms": acc_avg_ms,
                      "launches": acc_n,

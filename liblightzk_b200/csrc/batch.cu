@@ -6,7 +6,7 @@
 // once for the whole batch:
 //   gather bases -> digit count -> offset scan -> scatter -> accumulate
 //   -> fix-up -> bucket reduction (one level chain per window width) ->
-//   window combination (one thread per MSM)
+//   window combination (one warp per MSM)
 // so 64 MSMs cost about the launches of one.  MSMs are ordered by window
 // width so that the windows of equal width are contiguous and reduce
 // together.  NTTs are grouped by (size, direction) and each group is one
@@ -112,21 +112,25 @@ __global__ void k_bdigits(const BDesc* __restrict__ d, const uint64_t* __restric
     }
 }
 
-// Horner over each MSM's windows, one thread per MSM
+// Horner over each MSM's windows: one warp per MSM (<<<count, 32>>>) with
+// warp-uniform point operations, so the chain of about W * c doublings costs
+// one product per stage instead of a whole serial formula
 template <class F>
 __global__ void k_bfinish(const BDesc* __restrict__ d, uint32_t count, const XYZZ<F>* __restrict__ wres)
 {
-    for (uint64_t k = gtid(); k < count; k += gstride()) {
-        const BDesc& m = d[k];
-        XYZZ<F> r = xyzz_inf<F>();
+    const uint32_t k = blockIdx.x;
+    if (k >= count || threadIdx.x >= 32) return;
+    const BDesc& m = d[k];
+    XYZZ<F> r = xyzz_inf<F>();
+    if (m.n) {
         for (int w = (int)m.W - 1; w >= 0; w--) {
             if (w != (int)m.W - 1)
-                for (uint32_t b = 0; b < m.c; b++) r = xyzz_dbl_cold(r);
-            r = xyzz_add_cold(r, ld_elem(wres + m.win_base + w));
+                for (uint32_t b = 0; b < m.c; b++) r = xyzz_dbl_warp(r);
+            r = xyzz_add_warp(r, ld_elem(wres + m.win_base + w));
         }
-        if (m.n == 0) r = xyzz_inf<F>();
-        st_elem(reinterpret_cast<Jac<F>*>(m.out), xyzz_to_jac(r));
     }
+    Jac<F> j = xyzz_to_jac_warp(r);
+    if (threadIdx.x == 0) st_elem(reinterpret_cast<Jac<F>*>(m.out), j);
 }
 
 template <class F>
@@ -136,15 +140,20 @@ static int run_plan(lzk_batch_plan* p, cudaStream_t st)
     uint32_t count = (uint32_t)p->msm.size();
     if (count && p->total_pts) {
         unsigned g = grid_for(p->total_pts, 256, sm_count() * 16);
+        void* tr = trace_begin("batch_msm_sort", st);
         k_bgather<F><<<g, 256, 0, st>>>(p->d_desc, p->d_ptsoff, count, p->total_pts, static_cast<Aff<F>*>(p->bases)); note_launch();
         LZK_CUDA(cudaMemsetAsync(p->cnt, 0, sizeof(uint32_t) * p->total_buckets, st));
         k_bdigits<false><<<g, 256, 0, st>>>(p->d_desc, p->d_ptsoff, count, p->total_pts, p->off, p->cnt, p->ent); note_launch();
         LZK_TRY(scan_offsets(p->cnt, (uint32_t)p->total_buckets, p->off, p->bsums, st));
         k_bdigits<true><<<g, 256, 0, st>>>(p->d_desc, p->d_ptsoff, count, p->total_pts, p->off, p->cnt, p->ent); note_launch();
+        trace_end(tr, st);
         X* bsum = static_cast<X*>(p->bsum);
+        tr = trace_begin("batch_msm_accumulate", st);
         k_accumulate<F, LZK_BASES_AFFINE><<<grid_for(p->chunks, 128), 128, 0, st>>>(
             p->bases, p->ent, p->off, (uint32_t)p->total_buckets, p->chunks, bsum, static_cast<X*>(p->head),
             static_cast<X*>(p->tail)); note_launch();
+        trace_end(tr, st);
+        tr = trace_begin("batch_msm_fixup", st);
         LZK_CUDA(cudaMemsetAsync(p->large, 0, sizeof(uint32_t), st));
         k_fixup<F><<<grid_for(p->total_buckets, 256, sm_count() * 8), 256, 0, st>>>(p->off, (uint32_t)p->total_buckets, bsum,
                                                                             static_cast<X*>(p->head),
@@ -152,7 +161,9 @@ static int run_plan(lzk_batch_plan* p, cudaStream_t st)
         constexpr unsigned fx_threads = 32768 / sizeof(X);
         k_fixup_large<F><<<sm_count() * 2, fx_threads, fx_threads * sizeof(X), st>>>(p->off, bsum, static_cast<X*>(p->head),
                                                                              static_cast<X*>(p->tail), p->large); note_launch();
+        trace_end(tr, st);
         // one bucket reduction per window width
+        tr = trace_begin("batch_msm_reduce", st);
         uint64_t wdone = 0;
         for (auto& wg : p->wgroups) {
             LZK_TRY(reduce_buckets<F>(bsum + wg.bucket_base, p->off + wg.bucket_base, (uint32_t)wg.windows,
@@ -161,9 +172,12 @@ static int run_plan(lzk_batch_plan* p, cudaStream_t st)
                                       static_cast<X*>(p->wres) + wdone, st));
             wdone += wg.windows;
         }
-        k_bfinish<F><<<grid_for(count, 32), 32, 0, st>>>(p->d_desc, count, static_cast<const X*>(p->wres)); note_launch();
-    } else if (count) {
-        k_bfinish<F><<<grid_for(count, 32), 32, 0, st>>>(p->d_desc, count, static_cast<const X*>(p->wres)); note_launch();
+        trace_end(tr, st);
+    }
+    if (count) {
+        void* tr = trace_begin("batch_msm_finish", st);
+        k_bfinish<F><<<count, 32, 0, st>>>(p->d_desc, count, static_cast<const X*>(p->wres)); note_launch();
+        trace_end(tr, st);
     }
     return launch_status();
 }
@@ -173,7 +187,9 @@ static int run_all(lzk_batch_plan* p, cudaStream_t st)
     if (!p->ngroups.empty()) {
         LZK_CUDA(cudaEventRecord(p->ev_fork, st));
         LZK_CUDA(cudaStreamWaitEvent(p->s_ntt, p->ev_fork, 0));
+        void* tr = trace_begin("batch_ntt", p->s_ntt);
         for (auto& g : p->ngroups) LZK_TRY(ntt_run(nullptr, g.k, g.dir, g.count, 0, nullptr, p->s_ntt, g.ptrs));
+        trace_end(tr, p->s_ntt);
         LZK_CUDA(cudaEventRecord(p->ev_join, p->s_ntt));
     }
     LZK_TRY(p->group == 2 ? run_plan<Fq2>(p, st) : run_plan<Fq>(p, st));

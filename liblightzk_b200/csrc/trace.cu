@@ -60,6 +60,13 @@ void* trace_begin(const char* name, cudaStream_t st)
             ev = hit;
         }
     }
+    if (ev) {
+        // no timing events inside a stream capture: the graph would keep
+        // recording into events that are destroyed once resolved
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) { cudaGetLastError(); ev = false; }
+        else if (cs != cudaStreamCaptureStatusNone) ev = false;
+    }
     if (!ev && !nv) return nullptr;
     TraceRec* r = new TraceRec{name, nullptr, nullptr, 0, ev};
     if (nv) r->nvtx = nvtxRangeStartA(name);
