@@ -57,6 +57,7 @@ def parse():
     ap.add_argument("--plain", action="store_true", help="msm cases: plain affine bases instead of a shifted table")
     ap.add_argument("--inflight", type=int, default=4)
     ap.add_argument("--requests", type=int, default=48)
+    ap.add_argument("--tune-out", default=None, help="batch case: save the measured tuning table (JSON) here")
     return ap.parse_args()
 
 
@@ -277,7 +278,12 @@ def run_batch_case(args):
     import torch
 
     from liblightzk_b200 import autotune, batch, msm, ntt
-    tuned = autotune.tune(1, log_ns=range(10, 21), spread=2, reps=2)
+    # the tuning table for this workload's size classes, measured here: window
+    # width with reduction run, accumulation chunk, NTT pass block
+    tuned = autotune.tune_msm(1, log_ns=range(10, 21), spread=2, reps=2)
+    tuned_ntt = autotune.tune_ntt(range(12, 23), reps=2)
+    if args.tune_out:
+        autotune.save(args.tune_out)
     msms, ntts, _pool = batch.workload_config3()
     plan = batch.BatchPlan(1, msms, ntts)
     stream = torch.cuda.Stream()
@@ -321,7 +327,9 @@ def run_batch_case(args):
                       "ntt_elements": elems, "plan_graph_ms": plan_ms, "one_by_one_ms": seq_ms,
                       "speedup": float(np.median(seq_ms) / np.median(plan_ms)),
                       "plan_device_bytes": plan.device_bytes(), "phases_ms_eager": phases,
-                      "tuned_windows": {lg: v[0] for lg, v in tuned.items()}}), flush=True)
+                      "tuned_table": {"msm_g1": {lg: {k: v[k] for k in ("window", "run", "chunk")}
+                                                 for lg, v in tuned.items()},
+                                      "ntt_block": {lg: v[0] for lg, v in tuned_ntt.items()}}}), flush=True)
 
 
 def run_serve_case(args):

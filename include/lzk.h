@@ -122,6 +122,12 @@ typedef struct lzk_msm_cfg {
     void* workspace;          /* optional device scratch; NULL = allocate
                                  stream-ordered from the device pool        */
     size_t workspace_bytes;
+    uint32_t acc_chunk;       /* sorted bucket entries one accumulation
+                                 thread adds (power of two, 8..512);
+                                 0 = the tuning table (default 64)          */
+    uint32_t reduce_run;      /* buckets per lane run in the bucket-
+                                 reduction tiles (power of two, 1..16); 0 =
+                                 the tuning table (default 4)               */
 } lzk_msm_cfg;
 
 int lzk_msm_g1(const lzk_fr_t* scalars, const void* bases, size_t n,
@@ -424,10 +430,31 @@ int lzk_batch_plan_run(lzk_batch_plan* plan, int use_graph, void* stream);
 size_t lzk_batch_plan_device_bytes(const lzk_batch_plan* plan);
 int lzk_batch_plan_destroy(lzk_batch_plan* plan);
 
-/* Autotuner table: the window width plain-base MSMs of about 2^log_n points
- * use when their cfg asks for autotuning (window_bits = 0 clears the entry
- * and falls back to the cost model).  Filled from timings by
+/* Tuning table.  Per knob, group (1 = G1, 2 = G2; ignored for NTT knobs)
+ * and size class log_n = ceil(log2 n), the value an operator uses when its
+ * configuration leaves it open:
+ *   LZK_TUNE_MSM_WINDOW      window width of plain-base MSMs (cfg
+ *                            window_bits = 0); unset: the cost model
+ *   LZK_TUNE_MSM_CHUNK       sorted entries per accumulation thread (cfg
+ *                            acc_chunk = 0), 8..512, power of two; unset: 64
+ *   LZK_TUNE_MSM_REDUCE_RUN  buckets per lane run in the reduction tiles
+ *                            (cfg reduce_run = 0), 1..16; unset: 4
+ *   LZK_TUNE_NTT_BLOCK       elements per block of an NTT pass (the stages
+ *                            a pass runs in shared memory), 256..4096, power
+ *                            of two; unset: 2048
+ * The reference fixes all of these at compile time (c = 12 with 4096
+ * buckets, msm.cuh:216-227; one launch per NTT stage, poly.cuh:42-63).
+ * value 0 clears an entry.  A Groth16 prover and a batch plan read the table
+ * once, when they are created.  Filled from device timings by
  * liblightzk_b200.autotune. */
+#define LZK_TUNE_MSM_WINDOW     0
+#define LZK_TUNE_MSM_CHUNK      1
+#define LZK_TUNE_MSM_REDUCE_RUN 2
+#define LZK_TUNE_NTT_BLOCK      3
+int lzk_tune_set(int knob, int group, uint32_t log_n, uint32_t value);
+/* The value in effect (the entry, or the default; 0 for an unset window). */
+uint32_t lzk_tune_get(int knob, int group, uint32_t log_n);
+/* lzk_tune_set(LZK_TUNE_MSM_WINDOW, group, log_n, window_bits). */
 int lzk_msm_set_window(int group, uint32_t log_n, uint32_t window_bits);
 
 /* ------------------------------------------------------------ tracing

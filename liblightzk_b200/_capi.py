@@ -65,6 +65,8 @@ SIGNATURES = {
     "lzk_batch_plan_device_bytes": (c_sz, [c_p]),
     "lzk_batch_plan_destroy": (c_i, [c_p]),
     "lzk_msm_set_window": (c_i, [c_i, c_u32, c_u32]),
+    "lzk_tune_set": (c_i, [c_i, c_i, c_u32, c_u32]),
+    "lzk_tune_get": (c_u32, [c_i, c_i, c_u32]),
     "lzk_trace_enable": (None, [c_i]),
     "lzk_trace_nvtx": (None, [c_i]),
     "lzk_trace_reset": (None, []),
@@ -89,6 +91,8 @@ class MsmCfg(ctypes.Structure):
         ("level_stride", ctypes.c_size_t),
         ("workspace", ctypes.c_void_p),
         ("workspace_bytes", ctypes.c_size_t),
+        ("acc_chunk", ctypes.c_uint32),
+        ("reduce_run", ctypes.c_uint32),
     ]
 
 

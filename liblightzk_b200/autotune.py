@@ -1,14 +1,28 @@
-"""Measured window-width autotuner for plain-base MSMs.
+"""Measured autotuner for the library's tuning table (lzk_tune_set).
 
-For each size class 2^log_n the tuner times the cost model's window width
-and its neighbours on the device (CUDA events, random inputs, median of a few
-runs) and installs the fastest in the library's table (lzk_msm_set_window),
-which every autotuned MSM and batch plan then uses.
+Per size class 2^log_n it times candidates on the device (CUDA events,
+seeded random inputs, median of a few runs) and installs the fastest:
+
+  window  Pippenger window width of plain-base MSMs (the cost model's
+          width and its neighbours)
+  chunk   sorted bucket entries one accumulation thread adds (32, 64, 128)
+  run     buckets per lane run in the bucket-reduction tiles (4, 8, 16)
+  ntt     elements per block of an NTT pass, i.e. how a transform's stages
+          split into passes (1024, 2048, 4096)
+
+Every autotuned MSM, batch plan and prover made afterwards uses the table
+(a prover or plan reads it when it is created).  `save` / `load` keep a
+table as JSON, so a tuned table can be reused without re-timing.
 """
+import json
+
 import numpy as np
 import torch
 
-from . import _capi, msm, synth
+from . import _capi, msm, ntt, synth
+
+WINDOW, CHUNK, RUN, NTT_BLOCK = 0, 1, 2, 3
+KNOBS = {"window": WINDOW, "chunk": CHUNK, "run": RUN, "ntt": NTT_BLOCK}
 
 
 def _time(fn, reps):
@@ -23,15 +37,23 @@ def _time(fn, reps):
     return float(np.median(ts[1:]))
 
 
+def set_value(knob, group, log_n, value):
+    _capi.call("lzk_tune_set", KNOBS[knob], group, log_n, value)
+
+
+def get_value(knob, group, log_n):
+    return int(_capi.lib().lzk_tune_get(KNOBS[knob], group, log_n))
+
+
 def tune(group=1, log_ns=range(10, 21), spread=2, reps=3, seed=11, install=True):
-    """returns {log_n: (best_c, {c: ms})}"""
+    """window widths only: {log_n: (best_c, {c: ms})}"""
     table = {}
     top = max(log_ns)
     sc_all = synth.random_fr(1 << top, seed, 90)
     bases_all = synth.fixed_base(group, synth.random_fr(1 << top, seed, 91))
     for lg in log_ns:
         n = 1 << lg
-        _capi.call("lzk_msm_set_window", group, lg, 0)      # model value as the centre
+        set_value("window", group, lg, 0)      # model value as the centre
         c0 = msm.autotune_window(group, n)
         res = {}
         for c in range(max(2, c0 - spread), min(22, c0 + spread) + 1):
@@ -39,5 +61,82 @@ def tune(group=1, log_ns=range(10, 21), spread=2, reps=3, seed=11, install=True)
         best = min(res, key=res.get)
         table[lg] = (best, res)
         if install:
-            _capi.call("lzk_msm_set_window", group, lg, best)
+            set_value("window", group, lg, best)
     return table
+
+
+def tune_msm(group=1, log_ns=range(10, 21), spread=2, reps=3, seed=11, chunks=(32, 64, 128), runs=(4, 8, 16)):
+    """per size class: window width and reduction run together (the run
+    sets how much each bucket costs, which moves the best width), then the
+    accumulation chunk at that pair; installs them and returns
+    {log_n: {"window": best_c, "run": best_run, "chunk": best_chunk,
+             "ms": {"c,run": ms}, "chunk_ms": {chunk: ms}}}"""
+    out = {}
+    top = max(log_ns)
+    sc_all = synth.random_fr(1 << top, seed, 90)
+    bases_all = synth.fixed_base(group, synth.random_fr(1 << top, seed, 91))
+    for lg in log_ns:
+        n = 1 << lg
+        s, b = sc_all[:n], bases_all[:n]
+        for k in ("window", "chunk", "run"):
+            set_value(k, group, lg, 0)
+        c0 = msm.autotune_window(group, n)
+        res = {}
+        for c in range(max(2, c0 - spread), min(22, c0 + spread) + 1):
+            for r in runs:
+                set_value("run", group, lg, r)
+                res[(c, r)] = _time(lambda c=c: msm.msm(group, s, b, window_bits=c), reps)
+        c_best, r_best = min(res, key=res.get)
+        set_value("window", group, lg, c_best)
+        set_value("run", group, lg, r_best)
+        cres = {}
+        for v in chunks:
+            set_value("chunk", group, lg, v)
+            cres[v] = _time(lambda: msm.msm(group, s, b), reps)
+        ch_best = min(cres, key=cres.get)
+        set_value("chunk", group, lg, ch_best)
+        out[lg] = {"window": c_best, "run": r_best, "chunk": ch_best,
+                   "ms": {f"{c},{r}": v for (c, r), v in res.items()}, "chunk_ms": cres}
+    return out
+
+
+def tune_ntt(log_ns=range(12, 23), reps=3, seed=12, blocks=(1024, 2048, 4096), direction=ntt.COSET_FORWARD):
+    """NTT block size per transform size; installs the fastest and returns
+    {log_n: (best, {block: ms})}"""
+    out = {}
+    for lg in log_ns:
+        x = synth.random_fr(1 << lg, seed, 92)
+        ntt.prepare(lg)
+        res = {}
+        for v in blocks:
+            set_value("ntt", 0, lg, v)
+            res[v] = _time(lambda: ntt.ntt(x, lg, direction), reps)
+        best = min(res, key=res.get)
+        set_value("ntt", 0, lg, best)
+        out[lg] = (best, res)
+    return out
+
+
+def current(groups=(1, 2), log_ns=range(0, 33)):
+    """the installed table as a JSON-able dict of non-default entries"""
+    t = {"msm": {}, "ntt": {}}
+    for g in groups:
+        t["msm"][str(g)] = {k: {str(lg): get_value(k, g, lg) for lg in log_ns} for k in ("window", "chunk", "run")}
+    t["ntt"] = {str(lg): get_value("ntt", 0, lg) for lg in log_ns}
+    return t
+
+
+def save(path, table=None):
+    with open(path, "w") as f:
+        json.dump(table or current(), f, indent=1, sort_keys=True)
+
+
+def load(path):
+    """install a table written by save()"""
+    t = json.load(open(path))
+    for g, knobs in t.get("msm", {}).items():
+        for k, vals in knobs.items():
+            for lg, v in vals.items():
+                set_value(k, int(g), int(lg), int(v))
+    for lg, v in t.get("ntt", {}).items():
+        set_value("ntt", 0, int(lg), int(v))

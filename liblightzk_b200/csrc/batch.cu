@@ -39,6 +39,7 @@ struct lzk_batch_plan {
     struct NGroup { uint32_t k; int dir; uint32_t count; lzk::Fr** ptrs; };
     std::vector<NGroup> ngroups;
     uint64_t total_pts = 0, total_buckets = 0, total_windows = 0, max_entries = 0, chunks = 0, lvl = 0;
+    uint32_t chunk = 0, run = 0;       // accumulation chunk, reduction run (tuning table, at creation)
     char* ws = nullptr;
     size_t ws_bytes = 0;
     BDesc* d_desc = nullptr;
@@ -150,16 +151,16 @@ static int run_plan(lzk_batch_plan* p, cudaStream_t st)
         X* bsum = static_cast<X*>(p->bsum);
         tr = trace_begin("batch_msm_accumulate", st);
         k_accumulate<F, LZK_BASES_AFFINE><<<grid_for(p->chunks, 128), 128, 0, st>>>(
-            p->bases, p->ent, p->off, (uint32_t)p->total_buckets, p->chunks, bsum, static_cast<X*>(p->head),
+            p->bases, p->ent, p->off, (uint32_t)p->total_buckets, p->chunks, p->chunk, bsum, static_cast<X*>(p->head),
             static_cast<X*>(p->tail)); note_launch();
         trace_end(tr, st);
         tr = trace_begin("batch_msm_fixup", st);
         LZK_CUDA(cudaMemsetAsync(p->large, 0, sizeof(uint32_t), st));
-        k_fixup<F><<<grid_for(p->total_buckets, 256, sm_count() * 8), 256, 0, st>>>(p->off, (uint32_t)p->total_buckets, bsum,
+        k_fixup<F><<<grid_for(p->total_buckets, 256, sm_count() * 8), 256, 0, st>>>(p->off, (uint32_t)p->total_buckets, p->chunk, bsum,
                                                                             static_cast<X*>(p->head),
                                                                             static_cast<X*>(p->tail), p->large); note_launch();
         constexpr unsigned fx_threads = 32768 / sizeof(X);
-        k_fixup_large<F><<<sm_count() * 2, fx_threads, fx_threads * sizeof(X), st>>>(p->off, bsum, static_cast<X*>(p->head),
+        k_fixup_large<F><<<sm_count() * 2, fx_threads, fx_threads * sizeof(X), st>>>(p->off, p->chunk, bsum, static_cast<X*>(p->head),
                                                                              static_cast<X*>(p->tail), p->large); note_launch();
         trace_end(tr, st);
         // one bucket reduction per window width
@@ -169,7 +170,7 @@ static int run_plan(lzk_batch_plan* p, cudaStream_t st)
             LZK_TRY(reduce_buckets<F>(bsum + wg.bucket_base, p->off + wg.bucket_base, (uint32_t)wg.windows,
                                       1u << (wg.c - 1), static_cast<X*>(p->lr[0]), static_cast<X*>(p->la[0]),
                                       static_cast<X*>(p->lr[1]), static_cast<X*>(p->la[1]),
-                                      static_cast<X*>(p->wres) + wdone, st));
+                                      static_cast<X*>(p->wres) + wdone, st, p->run));
             wdone += wg.windows;
         }
         trace_end(tr, st);
@@ -250,7 +251,12 @@ static int create_plan(const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_des
     }
     if (p->total_pts >= (1ull << 31) || p->total_buckets >= (1ull << 32) - 1 || p->max_entries >= (1ull << 32))
         return LZK_EINVAL;
-    p->chunks = (p->max_entries + kAccChunk - 1) / kAccChunk;
+    // the plan's largest MSM picks the accumulation chunk and reduction run
+    size_t largest = 0;
+    for (size_t i = 0; i < n_msm; i++) largest = std::max(largest, msms[i].n);
+    p->chunk = tune_chunk(p->group, largest);
+    p->run = tune_run(p->group, largest);
+    p->chunks = (p->max_entries + p->chunk - 1) / p->chunk;
     for (auto& g : p->wgroups) {
         uint64_t nb = 1ull << (g.c - 1);
         p->lvl = std::max<uint64_t>(p->lvl, g.windows * (nb > kLevelL ? nb / kLevelL : 1));

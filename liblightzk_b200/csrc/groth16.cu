@@ -165,6 +165,18 @@ static Scal to_scal(const lzk_fr_t* f)
     return s;
 }
 
+lzk_msm_cfg prover_msm_cfg(const lzk_prover* p, int i, size_t level_stride)
+{
+    lzk_msm_cfg cfg{};
+    cfg.window_bits = p->c;
+    cfg.flags = LZK_MSM_PRECOMPUTED;
+    cfg.precomp_windows = p->wins;
+    cfg.level_stride = level_stride;
+    cfg.acc_chunk = p->chunk[i];
+    cfg.reduce_run = p->run[i];
+    return cfg;
+}
+
 template <class T>
 static int dalloc(size_t* acct, T** ptr, size_t count)
 {
@@ -205,13 +217,9 @@ int ctx_create(const lzk_prover* p, bool serving, ProveCtx** out)
         if ((rc = dalloc(&x->bytes, &x->sm1, 6))) break;
         if ((rc = dalloc(&x->bytes, &x->sm2, 1))) break;
         for (int i = 0; i < 3 && rc == LZK_OK; i++) {
-            lzk_msm_cfg cfg{};
-            cfg.window_bits = p->c;
-            cfg.flags = LZK_MSM_PRECOMPUTED;
-            cfg.precomp_windows = p->wins;
             // ws[0]: the concatenated L and H MSM; ws[1]: A and B1; ws[2]: B2
             size_t n = i == 0 ? p->tn[2] : p->n_vars;
-            cfg.level_stride = n;
+            lzk_msm_cfg cfg = prover_msm_cfg(p, i, n);
             x->wsb[i] = lzk_msm_workspace_bytes(i == 2 ? 2 : 1, n, &cfg);
             rc = dalloc(&x->bytes, reinterpret_cast<char**>(&x->ws[i]), x->wsb[i]);
         }
@@ -276,6 +284,12 @@ static int create(const lzk_groth16_circuit* c, const lzk_groth16_pk* pk, int mo
     p->tn[0] = p->tn[1] = c->n_vars;
     p->nl = c->n_vars - c->n_public - 1;
     p->tn[2] = p->nl + (p->M - 1);
+    for (int i = 0; i < 3; i++) {
+        size_t n = i == 0 ? p->tn[2] : p->n_vars;
+        int group = i == 2 ? 2 : 1;
+        p->chunk[i] = tune_chunk(group, n);
+        p->run[i] = tune_run(group, n);
+    }
 
     LZK_TRY(ctx_create(p, false, &p->ctx0));
     cudaStream_t st = p->ctx0->s1;
@@ -346,11 +360,7 @@ static int create(const lzk_groth16_circuit* c, const lzk_groth16_pk* pk, int mo
 static int msm_tab1(const lzk_prover* p, ProveCtx* x, int q, const Fr* scal, size_t n, Jac<Fq>* out, int wsi,
                     cudaStream_t st, bool presorted = false)
 {
-    lzk_msm_cfg cfg{};
-    cfg.window_bits = p->c;
-    cfg.flags = LZK_MSM_PRECOMPUTED;
-    cfg.precomp_windows = p->wins;
-    cfg.level_stride = p->tn[q];
+    lzk_msm_cfg cfg = prover_msm_cfg(p, wsi, p->tn[q]);
     cfg.workspace = x->ws[wsi];
     cfg.workspace_bytes = x->wsb[wsi];
     if (presorted) return msm_g1_presorted(scal, p->tab[q], n, out, &cfg, st, x->zs_off, x->zs_ent);
@@ -388,11 +398,7 @@ int prove_ctx(const lzk_prover* p, ProveCtx* x, const Fr* z, const lzk_fr_t* r, 
     LZK_CUDA(cudaEventRecord(x->ev_sorted, x->s1));
     LZK_CUDA(cudaStreamWaitEvent(x->s2, x->ev_sorted, 0));
     {
-        lzk_msm_cfg cfg{};
-        cfg.window_bits = p->c;
-        cfg.flags = LZK_MSM_PRECOMPUTED;
-        cfg.precomp_windows = p->wins;
-        cfg.level_stride = p->tn2;
+        lzk_msm_cfg cfg = prover_msm_cfg(p, 2, p->tn2);
         cfg.workspace = x->ws[2];
         cfg.workspace_bytes = x->wsb[2];
         LZK_TRY(msm_g2_presorted(z, p->tab2, p->n_vars, x->g2res, &cfg, x->s2, x->zs_off, x->zs_ent));
@@ -452,11 +458,7 @@ int prove_ctx(const lzk_prover* p, ProveCtx* x, const Fr* z, const lzk_fr_t* r, 
     // L and H as one MSM: scalars z_(n_public+1) .. z_(n_vars-1), then the
     // H coefficients, over the concatenated table
     {
-        lzk_msm_cfg cfg{};
-        cfg.window_bits = p->c;
-        cfg.flags = LZK_MSM_PRECOMPUTED;
-        cfg.precomp_windows = p->wins;
-        cfg.level_stride = p->tn[2];
+        lzk_msm_cfg cfg = prover_msm_cfg(p, 0, p->tn[2]);
         cfg.workspace = x->ws[0];
         cfg.workspace_bytes = x->wsb[0];
         LZK_TRY(msm_g1_concat(z + p->n_public + 1, p->nl, hs, p->M - 1, p->tab[2], x->g1res + 2, &cfg, st));

@@ -3,14 +3,14 @@
 #pragma once
 #include "common.cuh"
 #include "curve.cuh"
+#include "tune.cuh"
 
 namespace lzk {
 
 struct G1 { using F = Fq; };
 struct G2 { using F = Fq2; };
 
-constexpr uint32_t kAccChunk = 64;   // sorted entries per accumulation thread
-constexpr uint32_t kLevelL = 32;     // buckets per warp tile of the bucket reduction
+constexpr uint32_t kLevelL = 32;     // smallest warp tile of the bucket reduction (scratch bound)
 constexpr uint32_t kFixSmall = 64;   // partials a single fix-up thread folds
 
 struct MsmPlan {
@@ -23,6 +23,8 @@ struct MsmPlan {
     bool shared = false;   // precomputed table: one bucket set for all windows
     size_t stride = 0;     // table level stride
     size_t max_entries = 0;
+    uint32_t chunk = 0;    // sorted entries per accumulation thread
+    uint32_t run = 0;      // buckets per lane run of the reduction tiles
     size_t chunks = 0;
     // workspace offsets
     size_t o_cnt, o_off, o_ent, o_bsum, o_head, o_tail, o_lr0, o_la0, o_lr1, o_la1, o_scan, o_large, bytes;
@@ -30,8 +32,20 @@ struct MsmPlan {
 
 inline uint32_t windows_for(uint32_t c) { return (255 + c - 1) / c; }
 
+// accumulation chunk and reduction run of an MSM of n points in group g:
+// cfg's values, else the tuning table's
+inline uint32_t msm_chunk(const lzk_msm_cfg* cfg, int group, size_t n)
+{
+    return cfg && cfg->acc_chunk ? cfg->acc_chunk : tune_chunk(group, n);
+}
+inline uint32_t msm_run(const lzk_msm_cfg* cfg, int group, size_t n)
+{
+    return cfg && cfg->reduce_run ? cfg->reduce_run : tune_run(group, n);
+}
+
 template <class Gp>
-inline void plan_msm(MsmPlan& p, size_t n, uint32_t c, bool shared, size_t stride)
+inline void plan_msm(MsmPlan& p, size_t n, uint32_t c, bool shared, size_t stride, uint32_t chunk = kDefaultChunk,
+                     uint32_t run = kDefaultRun)
 {
     using X = XYZZ<typename Gp::F>;
     p.n = n; p.c = c; p.W = windows_for(c); p.nb = 1u << (c - 1);
@@ -39,7 +53,9 @@ inline void plan_msm(MsmPlan& p, size_t n, uint32_t c, bool shared, size_t strid
     p.wb = shared ? 1 : p.W;
     p.B = p.wb * p.nb;
     p.max_entries = n * (size_t)p.W;
-    p.chunks = (p.max_entries + kAccChunk - 1) / kAccChunk;
+    p.chunk = chunk;
+    p.run = run;
+    p.chunks = (p.max_entries + chunk - 1) / chunk;
     // bucket reduction scratch: wb * max(1, nb / kLevelL) points per buffer
     // (reduce_buckets)
     size_t lvl = (size_t)p.wb * (p.nb > kLevelL ? p.nb / kLevelL : 1);
@@ -151,15 +167,15 @@ __device__ __forceinline__ Aff<F> load_base(const void* bases, uint32_t v)
 template <class F, int LAYOUT>
 __global__ void __launch_bounds__(128, sizeof(F) == 32 ? 5 : 3) k_accumulate(const void* __restrict__ bases, const uint32_t* __restrict__ ent,
                                                     const uint32_t* __restrict__ off, uint32_t B, size_t chunks,
-                                                    XYZZ<F>* __restrict__ bsum, XYZZ<F>* __restrict__ head,
-                                                    XYZZ<F>* __restrict__ tail)
+                                                    uint32_t chunk, XYZZ<F>* __restrict__ bsum,
+                                                    XYZZ<F>* __restrict__ head, XYZZ<F>* __restrict__ tail)
 {
     uint64_t t = gtid();
     if (t >= chunks) return;
     uint32_t T = off[B];
-    uint64_t cs64 = t * kAccChunk;
+    uint64_t cs64 = t * chunk;
     if (cs64 >= T) return;
-    uint32_t cs = (uint32_t)cs64, ce = min(cs + kAccChunk, T);
+    uint32_t cs = (uint32_t)cs64, ce = (uint32_t)min((uint64_t)cs + chunk, (uint64_t)T);
     uint32_t b = bucket_of(off, 0, B, cs);
     uint32_t bbeg = off[b], bend = off[b + 1];
     XYZZ<F> acc = xyzz_inf<F>();
@@ -190,13 +206,13 @@ __global__ void __launch_bounds__(128, sizeof(F) == 32 ? 5 : 3) k_accumulate(con
 }
 
 template <class F>
-__global__ void k_fixup(const uint32_t* __restrict__ off, uint32_t B, XYZZ<F>* __restrict__ bsum,
+__global__ void k_fixup(const uint32_t* __restrict__ off, uint32_t B, uint32_t chunk, XYZZ<F>* __restrict__ bsum,
                         const XYZZ<F>* __restrict__ head, const XYZZ<F>* __restrict__ tail, uint32_t* __restrict__ large)
 {
     for (uint64_t b = gtid(); b < B; b += gstride()) {
         uint32_t s = off[b], e = off[b + 1];
         if (s == e) continue;
-        uint32_t c0 = s / kAccChunk, c1 = (e - 1) / kAccChunk;
+        uint32_t c0 = s / chunk, c1 = (e - 1) / chunk;
         if (c0 == c1) continue;
         if (c1 - c0 > kFixSmall) {
             large[1 + atomicAdd(large, 1u)] = (uint32_t)b;
@@ -211,7 +227,7 @@ __global__ void k_fixup(const uint32_t* __restrict__ off, uint32_t B, XYZZ<F>* _
 // One block per listed bucket: strided partial sums, then a tree in shared
 // memory.  Partial q of bucket b is tail[c0] (q = 0) or head[c0 + q].
 template <class F>
-__global__ void k_fixup_large(const uint32_t* __restrict__ off, XYZZ<F>* __restrict__ bsum,
+__global__ void k_fixup_large(const uint32_t* __restrict__ off, uint32_t chunk, XYZZ<F>* __restrict__ bsum,
                               const XYZZ<F>* __restrict__ head, const XYZZ<F>* __restrict__ tail,
                               const uint32_t* __restrict__ large)
 {
@@ -220,7 +236,7 @@ __global__ void k_fixup_large(const uint32_t* __restrict__ off, XYZZ<F>* __restr
     uint32_t nl = large[0];
     for (uint32_t idx = blockIdx.x; idx < nl; idx += gridDim.x) {
         uint32_t b = large[1 + idx];
-        uint32_t c0 = off[b] / kAccChunk, c1 = (off[b + 1] - 1) / kAccChunk;
+        uint32_t c0 = off[b] / chunk, c1 = (off[b + 1] - 1) / chunk;
         uint32_t np = c1 - c0 + 1;
         XYZZ<F> acc = xyzz_inf<F>();
         for (uint32_t q = threadIdx.x; q < np; q += blockDim.x)
@@ -332,10 +348,13 @@ struct RedShape {
     uint32_t r, L, lgL, P, lg;   // buckets per lane run, tile size, log2 L, tiles per set, log2 P
     uint32_t cT, cG, NP, NS;     // chunks of T, chunks of each G_i, partials and sums per set
 };
-inline RedShape red_shape(uint32_t m)
+// run: requested buckets per lane run (a power of two); a set too small
+// for 32 lanes of such runs takes shorter runs, down to single buckets
+inline RedShape red_shape(uint32_t m, uint32_t run = kDefaultRun)
 {
     RedShape s;
-    s.r = m >= 128 ? 4 : m >= 64 ? 2 : 1;
+    s.r = run ? run : 1;
+    while (s.r > 1 && 32 * s.r > m) s.r >>= 1;
     s.L = m < 32 * s.r ? m : 32 * s.r;
     s.lgL = 0; while ((1u << s.lgL) < s.L) s.lgL++;
     s.P = m / s.L;
@@ -415,9 +434,9 @@ __global__ void __launch_bounds__(128) k_red_combine(const XYZZ<F>* __restrict__
 // and scaled fit in the same size (NP, NS <= P).  win may alias R.
 template <class F>
 int reduce_buckets(const XYZZ<F>* bsum, const uint32_t* off, uint32_t wb, uint32_t m, XYZZ<F>* R, XYZZ<F>* T,
-                   XYZZ<F>* part, XYZZ<F>* scaled, XYZZ<F>* win, cudaStream_t st)
+                   XYZZ<F>* part, XYZZ<F>* scaled, XYZZ<F>* win, cudaStream_t st, uint32_t run = kDefaultRun)
 {
-    RedShape sh = red_shape(m);
+    RedShape sh = red_shape(m, run);
     k_red_tile<F><<<grid_for((size_t)wb * sh.P * 32, 128), 128, 0, st>>>(bsum, off, wb, m, sh.L, sh.r, R, T); note_launch();
     k_red_slices<F><<<grid_for((size_t)wb * sh.NP * 32, 128), 128, 0, st>>>(R, T, wb, sh, part); note_launch();
     k_red_scale<F><<<grid_for((size_t)wb * sh.NS * 32, 128), 128, 0, st>>>(part, wb, sh, scaled); note_launch();
@@ -477,8 +496,11 @@ int run_msm(const Fr* scalars, const void* bases, size_t n, Jac<typename Gp::F>*
         k_write_inf<F><<<1, 32, 0, st>>>(out); note_launch();
         return launch_status();
     }
+    const int group = sizeof(F) == 32 ? 1 : 2;
+    uint32_t chunk = msm_chunk(cfg, group, n), run = msm_run(cfg, group, n);
+    if (!tune_valid(LZK_TUNE_MSM_CHUNK, chunk) || !tune_valid(LZK_TUNE_MSM_REDUCE_RUN, run)) return LZK_EINVAL;
     MsmPlan p;
-    plan_msm<Gp>(p, n, c, shared, stride);
+    plan_msm<Gp>(p, n, c, shared, stride, chunk, run);
     void* tr_all = trace_begin(sizeof(F) == 32 ? "msm_g1" : "msm_g2", st);
     Scratch ws;
     LZK_TRY(ws.acquire(p.bytes, cfg ? cfg->workspace : nullptr, cfg ? cfg->workspace_bytes : 0, st));
@@ -506,18 +528,18 @@ int run_msm(const Fr* scalars, const void* bases, size_t n, Jac<typename Gp::F>*
         unsigned g = grid_for(p.chunks, 128);
         constexpr int REF = sizeof(F) == 32 ? (int)LZK_BASES_REF_G1_JAC : (int)LZK_BASES_REF_G2_LANES;
         if (layout == LZK_BASES_AFFINE) {
-            k_accumulate<F, LZK_BASES_AFFINE><<<g, 128, 0, st>>>(bases, ent, off, p.B, p.chunks, bsum, head, tail); note_launch();
+            k_accumulate<F, LZK_BASES_AFFINE><<<g, 128, 0, st>>>(bases, ent, off, p.B, p.chunks, p.chunk, bsum, head, tail); note_launch();
         } else {
-            k_accumulate<F, REF><<<g, 128, 0, st>>>(bases, ent, off, p.B, p.chunks, bsum, head, tail); note_launch();
+            k_accumulate<F, REF><<<g, 128, 0, st>>>(bases, ent, off, p.B, p.chunks, p.chunk, bsum, head, tail); note_launch();
         }
     }
     trace_end(tr, st);
     void* tr_fix = trace_begin(sizeof(F) == 32 ? "msm_g1_fixup" : "msm_g2_fixup", st);
     LZK_CUDA(cudaMemsetAsync(large, 0, sizeof(uint32_t), st));
-    k_fixup<F><<<grid_for(p.B, 256, sm_count() * 8), 256, 0, st>>>(off, p.B, bsum, head, tail, large); note_launch();
+    k_fixup<F><<<grid_for(p.B, 256, sm_count() * 8), 256, 0, st>>>(off, p.B, p.chunk, bsum, head, tail, large); note_launch();
     {
         constexpr unsigned fx_threads = 32768 / sizeof(X);   // 32 KB of shared memory
-        k_fixup_large<F><<<sm_count() * 2, fx_threads, fx_threads * sizeof(X), st>>>(off, bsum, head, tail, large); note_launch();
+        k_fixup_large<F><<<sm_count() * 2, fx_threads, fx_threads * sizeof(X), st>>>(off, p.chunk, bsum, head, tail, large); note_launch();
     }
     trace_end(tr_fix, st);
     LZK_TRY(launch_status());
@@ -525,7 +547,7 @@ int run_msm(const Fr* scalars, const void* bases, size_t n, Jac<typename Gp::F>*
     // weighted sums per bucket set
     void* tr_red = trace_begin(sizeof(F) == 32 ? "msm_g1_reduce" : "msm_g2_reduce", st);
     X* win = lr[0];
-    LZK_TRY(reduce_buckets<F>(bsum, off, p.wb, p.nb, lr[0], la[0], lr[1], la[1], win, st));
+    LZK_TRY(reduce_buckets<F>(bsum, off, p.wb, p.nb, lr[0], la[0], lr[1], la[1], win, st, p.run));
     void* tr_fin = trace_begin(sizeof(F) == 32 ? "msm_g1_finish" : "msm_g2_finish", st);
     k_finish<F><<<1, 32, 0, st>>>(win, p.wb, c, out); note_launch();
     trace_end(tr_fin, st);

@@ -22,7 +22,7 @@ int msm_g1_concat(const Fr* lo, size_t n_lo, const Fr* hi, size_t n_hi, const vo
     if (c < 2 || c > 24 || cfg->precomp_windows < windows_for(c) || cfg->level_stride < n) return LZK_EINVAL;
     if ((size_t)windows_for(c) * cfg->level_stride >= (1ull << 31)) return LZK_EINVAL;
     MsmPlan p;
-    plan_msm<G1>(p, n, c, true, cfg->level_stride);
+    plan_msm<G1>(p, n, c, true, cfg->level_stride, msm_chunk(cfg, 1, n), msm_run(cfg, 1, n));
     if (cfg->workspace_bytes < p.bytes) return LZK_EINVAL;
     // sort into the workspace at the offsets run_msm carves from it
     char* base = static_cast<char*>(cfg->workspace);

@@ -189,15 +189,13 @@ int msm_sort(const MsmPlan& p, const Fr* scalars, uint32_t* cnt, uint32_t* off, 
 // Cost model behind the default window width: mixed adds n*W(c) (8M+2S) plus
 // the reduction (two XYZZ adds per bucket, 12M+2S) plus, for plain bases,
 // the serial Horner doublings, weighted by their latency cost.
-// measured window widths by group and ceil(log2 n); 0 = use the model
-static uint8_t g_window_table[3][33];
-
+// measured window widths come from the tuning table (tune.cu), by group and
+// ceil(log2 n); an unset entry falls back to the model
 uint32_t msm_autotune(int group, size_t n, bool shared)
 {
     if (!shared && n && group >= 1 && group <= 2) {
-        uint32_t lg = 0;
-        while (lg < 32 && (size_t(1) << lg) < n) lg++;
-        if (g_window_table[group][lg]) return g_window_table[group][lg];
+        uint32_t w = tune_lookup(LZK_TUNE_MSM_WINDOW, group, n);
+        if (w) return w;
     }
     (void)group;
     if (n == 0) return 8;
@@ -238,13 +236,6 @@ using namespace lzk;
 
 extern "C" {
 
-int lzk_msm_set_window(int group, uint32_t log_n, uint32_t window_bits)
-{
-    if (group < 1 || group > 2 || log_n > 32 || (window_bits && (window_bits < 2 || window_bits > 24))) return LZK_EINVAL;
-    g_window_table[group][log_n] = (uint8_t)window_bits;
-    return LZK_OK;
-}
-
 uint32_t lzk_msm_precomp_windows(uint32_t window_bits) { return window_bits ? windows_for(window_bits) : 0; }
 
 uint32_t lzk_msm_autotune_window(int group, size_t n, uint32_t flags)
@@ -257,9 +248,11 @@ size_t lzk_msm_workspace_bytes(int group, size_t n, const lzk_msm_cfg* cfg)
     bool shared = cfg && (cfg->flags & LZK_MSM_PRECOMPUTED);
     uint32_t c = (cfg && cfg->window_bits) ? cfg->window_bits : msm_autotune(group, n, shared);
     if (c < 2 || c > 24 || n == 0) return 0;
+    uint32_t chunk = msm_chunk(cfg, group, n), run = msm_run(cfg, group, n);
+    if (!tune_valid(LZK_TUNE_MSM_CHUNK, chunk)) return 0;
     MsmPlan p;
-    if (group == 2) plan_msm<G2>(p, n, c, shared, cfg ? cfg->level_stride : 0);
-    else plan_msm<G1>(p, n, c, shared, cfg ? cfg->level_stride : 0);
+    if (group == 2) plan_msm<G2>(p, n, c, shared, cfg ? cfg->level_stride : 0, chunk, run);
+    else plan_msm<G1>(p, n, c, shared, cfg ? cfg->level_stride : 0, chunk, run);
     return p.bytes;
 }
 

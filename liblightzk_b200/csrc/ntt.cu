@@ -15,13 +15,13 @@
 // g^j first, g = 5 = Fr::multiplicative_generator, alt_bn128_init.cu:50);
 // coset inverse (inverse, then * g^-j).
 #include "ntt.cuh"
+#include "tune.cuh"
 #include <map>
 #include <mutex>
 
 namespace lzk {
 
 constexpr int kNttMaxLog = 26;
-constexpr uint32_t kNttElems = 2048;   // elements per block in a pass (64 KB smem)
 constexpr uint32_t kNttThreads = 256;
 constexpr uint32_t kPowLoBits = 12;    // g^j = lo[j & 4095] * hi[j >> 12]
 
@@ -260,8 +260,9 @@ int ntt_prepare_launch()
     LZK_CUDA(cudaGetDevice(&dev));
     std::lock_guard<std::mutex> g(mu);
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-        LZK_CUDA(cudaFuncSetAttribute(k_ntt_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttElems * sizeof(Fr)));
-        LZK_CUDA(cudaFuncSetAttribute(k_ntt_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNttElems * sizeof(Fr)));
+        // the largest block the tuning table allows (kMaxNttBlock elements)
+        LZK_CUDA(cudaFuncSetAttribute(k_ntt_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxNttBlock * sizeof(Fr)));
+        LZK_CUDA(cudaFuncSetAttribute(k_ntt_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxNttBlock * sizeof(Fr)));
         attr_set[dev] = true;
     }
     return LZK_OK;
@@ -272,7 +273,10 @@ int ntt_passes(Fr* data, uint32_t k, uint32_t count, size_t bstride, const Fr* t
 {
     if (k == 0 || k > 30 || count == 0 || count > 65535 || (!data && !ptrs) || !tw) return LZK_EINVAL;
     LZK_TRY(ntt_prepare_launch());
-    const uint32_t maxm = 11;
+    // block size from the tuning table: 2^maxm elements, at most maxm stages a pass
+    const uint32_t elems = tune_ntt_block(k);
+    uint32_t maxm = 0;
+    while ((1u << (maxm + 1)) <= elems) maxm++;
     const uint32_t P = (k + maxm - 1) / maxm;
     const size_t n = size_t(1) << k;
     uint32_t done = 0;   // stages done by earlier passes
@@ -284,7 +288,7 @@ int ntt_passes(Fr* data, uint32_t k, uint32_t count, size_t bstride, const Fr* t
         pp.lowbits = dit ? done : k - done - m;
         pp.s0 = dit ? 0 : done;
         uint32_t G = 1u << m;
-        uint32_t R = kNttElems / G;
+        uint32_t R = elems / G;
         if ((size_t)R > (n >> m)) R = (uint32_t)(n >> m);
         if (R == 0) R = 1;
         pp.R = R;

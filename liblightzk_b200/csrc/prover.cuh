@@ -5,6 +5,12 @@
 #include "curve.cuh"
 #include "r1cs.cuh"
 
+struct lzk_prover;
+namespace lzk {
+// the MSM configuration of the prover's workspace i (see lzk_prover::chunk)
+lzk_msm_cfg prover_msm_cfg(const lzk_prover* p, int i, size_t level_stride);
+}
+
 namespace lzk {
 
 // Scratch and streams of one proof in flight.  A prover owns one (used by
@@ -46,6 +52,10 @@ struct lzk_prover {
     lzk::Aff<lzk::Fq2>* tab2 = nullptr;
     size_t tn2 = 0;
     uint32_t c = 16, wins = 16;
+    // accumulation chunk and reduction run of the three MSM workspaces (0:
+    // the L + H MSM, 1: A and B1, 2: B2), read from the tuning table when
+    // the prover is made
+    uint32_t chunk[3] = {0, 0, 0}, run[3] = {0, 0, 0};
     // constants in device memory
     lzk::Aff<lzk::Fq>* g1c = nullptr;   // alpha1, beta1, delta1
     lzk::Aff<lzk::Fq2>* g2c = nullptr;  // beta2, delta2
