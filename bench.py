@@ -48,7 +48,8 @@ def parse():
     ap.add_argument("--matmul-p", type=int, default=100)
     ap.add_argument("--window", type=int, default=17)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", choices=["prove", "msm-g1", "msm-g2", "ntt", "spmv", "batch", "serve", "reference-gpu"],
+    ap.add_argument("--case", choices=["prove", "msm-g1", "msm-g2", "ntt", "spmv", "batch", "serve", "reference-gpu",
+                                       "tune"],
                     default="prove",
                     help="prove = the benchmark; msm-g1/msm-g2/ntt run one operator at --log-n for profiling; "
                          "reference-gpu times the reference's own GPU programs (built by make -C oracle refgpu)")
@@ -57,7 +58,10 @@ def parse():
     ap.add_argument("--plain", action="store_true", help="msm cases: plain affine bases instead of a shifted table")
     ap.add_argument("--inflight", type=int, default=4)
     ap.add_argument("--requests", type=int, default=48)
-    ap.add_argument("--tune-out", default=None, help="batch case: save the measured tuning table (JSON) here")
+    ap.add_argument("--tune-out", default=None, help="tune case: write the measured tuning table (JSON) here")
+    ap.add_argument("--retune", action="store_true", help="batch case: measure the tuning table instead of loading "
+                                                          "the packaged one")
+    ap.add_argument("--no-tuning-table", action="store_true", help="do not load the packaged tuning table")
     return ap.parse_args()
 
 
@@ -278,12 +282,14 @@ def run_batch_case(args):
     import torch
 
     from liblightzk_b200 import autotune, batch, msm, ntt
-    # the tuning table for this workload's size classes, measured here: window
-    # width with reduction run, accumulation chunk, NTT pass block
-    tuned = autotune.tune_msm(1, log_ns=range(10, 21), spread=2, reps=2)
-    tuned_ntt = autotune.tune_ntt(range(12, 23), reps=2)
-    if args.tune_out:
-        autotune.save(args.tune_out)
+    # the tuning table (window width, reduction run, accumulation chunk, NTT
+    # pass block): the packaged table measured on this GPU model, or measured
+    # here for this workload's size classes with --retune
+    table_src = None if args.retune else autotune.load_default()
+    if table_src is None:
+        autotune.tune_msm(1, log_ns=range(10, 21), spread=2, reps=2)
+        autotune.tune_ntt(range(12, 23), reps=2)
+        table_src = "measured in this run"
     msms, ntts, _pool = batch.workload_config3()
     plan = batch.BatchPlan(1, msms, ntts)
     stream = torch.cuda.Stream()
@@ -327,9 +333,11 @@ def run_batch_case(args):
                       "ntt_elements": elems, "plan_graph_ms": plan_ms, "one_by_one_ms": seq_ms,
                       "speedup": float(np.median(seq_ms) / np.median(plan_ms)),
                       "plan_device_bytes": plan.device_bytes(), "phases_ms_eager": phases,
-                      "tuned_table": {"msm_g1": {lg: {k: v[k] for k in ("window", "run", "chunk")}
-                                                 for lg, v in tuned.items()},
-                                      "ntt_block": {lg: v[0] for lg, v in tuned_ntt.items()}}}), flush=True)
+                      "tuning_table": table_src,
+                      "tuned": {"msm_g1": {lg: {k: autotune.get_value(k, 1, lg) for k in ("window", "run", "chunk")}
+                                           for lg in range(10, 21)},
+                                "ntt_block": {lg: autotune.get_value("ntt", 0, lg) for lg in range(12, 23)}}}),
+          flush=True)
 
 
 def run_serve_case(args):
@@ -429,11 +437,37 @@ def run_serve_case(args):
     print(json.dumps(out), flush=True)
 
 
+def run_tune_case(args):
+    """measure the whole tuning table on this GPU and write it (--tune-out):
+    plain-base MSM window, reduction run and chunk per size class (G1 and
+    G2), NTT pass block per transform size, and the chunk and run of the
+    benchmark prover's own MSMs, chosen by timing whole proofs"""
+    from liblightzk_b200 import autotune, groth16, synth
+    t0 = time.time()
+    t1 = autotune.tune_msm(1, log_ns=range(10, 22), spread=2, reps=2)
+    t2 = autotune.tune_msm(2, log_ns=range(10, 21), spread=1, reps=2)
+    tn = autotune.tune_ntt(range(10, 25), reps=2)
+    circ = synth.Circuit(args.log_m, seed=1)
+    pk = synth.ProvingKey(circ, seed=7)
+    tp = autotune.tune_prover(circ, pk, window_bits=args.window)
+    if args.tune_out:
+        autotune.save(args.tune_out)
+    print(json.dumps({"case": "tune", "seconds": time.time() - t0,
+                      "msm_g1": {lg: {k: v[k] for k in ("window", "run", "chunk")} for lg, v in t1.items()},
+                      "msm_g2": {lg: {k: v[k] for k in ("window", "run", "chunk")} for lg, v in t2.items()},
+                      "ntt_block": {lg: {"best": v[0], "ms": v[1]} for lg, v in tn.items()},
+                      "prover_ms_per_proof": {f"chunk {c}, run {r}": ms for (c, r), ms in tp.items()}}), flush=True)
+
+
 def run_case(args):
     """one operator at 2^log_n, `reps` times, for profiling (prints ms)"""
     import torch
 
-    from liblightzk_b200 import _capi, msm, ntt, synth
+    from liblightzk_b200 import _capi, autotune, msm, ntt, synth
+    if args.case == "tune":
+        return run_tune_case(args)
+    if not args.no_tuning_table:
+        autotune.load_default()
     if args.case == "batch":
         return run_batch_case(args)
     if args.case == "serve":
@@ -514,8 +548,9 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
-    from liblightzk_b200 import _capi, device, groth16, msm, synth
+    from liblightzk_b200 import _capi, autotune, device, groth16, msm, synth
     dev = f"cuda:{local}"
+    tuning = None if args.no_tuning_table else autotune.load_default()
     # ---------------- setup (untimed) ----------------
     if args.circuit == "matmul":
         circ = synth.MatMulCircuit(args.matmul_p, device=dev)
@@ -771,7 +806,8 @@ def main():
         "data": "synthetic (seeded R1CS, witness and proving key generated on the device)",
         "config": {"workload": workload, "constraints": M, "variables": circ.n_vars,
                    "public_inputs": circ.n_public, "prove_mode": args.mode, "msm_window_bits": args.window,
-                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (GB-scale key tables)"},
+                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (GB-scale key tables)",
+                   "tuning_table": os.path.relpath(tuning, ROOT) if tuning else "built-in defaults"},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                        "mean": float(np.mean(lat))},
         "g1_msm_2e20_ms": g1_ms, "g1_msm_2e20_plain_ms": g1_plain_ms,

@@ -496,6 +496,18 @@ int lzk_trace_timeline(lzk_trace_span* spans, size_t cap, size_t* count);
  * from the call that needed it, with everything it had allocated released);
  * a negative value turns the failures off.  Process-wide. */
 int lzk_debug_fail_allocations(long long after);
+/* Debug builds (liblzk_b200_debug.so, compiled with LZK_DEBUG_CHECKS): the
+ * digit sort, bucket accumulation and fix-up kernels check every index their
+ * inputs imply and, instead of an out-of-range read or write, set a bit of a
+ * device error word and skip the access.  lzk_debug_check_word returns the
+ * bits set since it was last cleared on the current device (bit 0: bucket
+ * index, 1: scatter slot, 2: base index of a sorted entry, 3: bucket offset,
+ * 4: fix-up partial), clearing them when clear != 0; always 0 in release
+ * builds, which lzk_debug_checks_enabled tells apart (1 = checks compiled
+ * in).  The reference's counterparts are its CUDA_DEBUG prints and device
+ * traps (device-utils.cuh:3, mont_t.cuh:1108). */
+uint32_t lzk_debug_check_word(int clear);
+int lzk_debug_checks_enabled(void);
 /* Number of kernels this library has launched so far (all devices). */
 uint64_t lzk_launch_count(void);
 /* Measured 32-bit integer multiply-add rate of the current device

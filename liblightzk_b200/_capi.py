@@ -77,6 +77,8 @@ SIGNATURES = {
     "lzk_probe_mont_rate": (c_i, [ctypes.POINTER(ctypes.c_double)]),
     "lzk_launch_count": (ctypes.c_uint64, []),
     "lzk_debug_fail_allocations": (c_i, [ctypes.c_longlong]),
+    "lzk_debug_check_word": (c_u32, [c_i]),
+    "lzk_debug_checks_enabled": (c_i, []),
 }
 
 

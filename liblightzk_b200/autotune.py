@@ -15,11 +15,15 @@ Every autotuned MSM, batch plan and prover made afterwards uses the table
 table as JSON, so a tuned table can be reused without re-timing.
 """
 import json
+import os
 
 import numpy as np
 import torch
 
 from . import _capi, msm, ntt, synth
+
+# measured tables shipped with the package, by GPU name
+DEFAULT_TABLES = {"B200": os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning", "b200.json")}
 
 WINDOW, CHUNK, RUN, NTT_BLOCK = 0, 1, 2, 3
 KNOBS = {"window": WINDOW, "chunk": CHUNK, "run": RUN, "ntt": NTT_BLOCK}
@@ -115,6 +119,47 @@ def tune_ntt(log_ns=range(12, 23), reps=3, seed=12, blocks=(1024, 2048, 4096), d
         set_value("ntt", 0, lg, best)
         out[lg] = (best, res)
     return out
+
+
+def tune_prover(circuit, pk, mode=0, window_bits=17, chunks=(32, 64), runs=(4, 8, 16), proofs=8, seed=13):
+    """accumulation chunk and reduction run of a Groth16 prover's own MSMs
+    (shifted-table MSMs over the circuit's variables, the L + H concatenation
+    and the G2 query), chosen by timing whole proofs; installs the best
+    pair for those size classes and returns {(chunk, run): ms per proof}"""
+    from . import device, groth16
+    z = circuit.witness(seed)
+    rs = device.to_host(synth.random_fr(2, seed, 93))
+    nl = circuit.n_vars - circuit.n_public - 1
+    classes = {1: {int(np.ceil(np.log2(circuit.n_vars))), int(np.ceil(np.log2(nl + circuit.M - 1)))},
+               2: {int(np.ceil(np.log2(circuit.n_vars)))}}
+
+    def install(chunk, run):
+        for g, lgs in classes.items():
+            for lg in lgs:
+                set_value("chunk", g, lg, chunk)
+                set_value("run", g, lg, run)
+
+    res = {}
+    for chunk in chunks:
+        for run in runs:
+            install(chunk, run)
+            p = groth16.Prover(circuit, pk, mode=mode, window_bits=window_bits)
+            res[(chunk, run)] = _time(lambda: [p.prove(z, rs[0], rs[1]) for _ in range(proofs)], 2) / proofs
+            p.close()
+    best = min(res, key=res.get)
+    install(*best)
+    return res
+
+
+def load_default():
+    """install the packaged table measured on this GPU model, if there is
+    one; returns its path or None"""
+    name = torch.cuda.get_device_name()
+    for key, path in DEFAULT_TABLES.items():
+        if key in name and os.path.exists(path):
+            load(path)
+            return path
+    return None
 
 
 def current(groups=(1, 2), log_ns=range(0, 33)):

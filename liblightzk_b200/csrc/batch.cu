@@ -151,12 +151,12 @@ static int run_plan(lzk_batch_plan* p, cudaStream_t st)
         X* bsum = static_cast<X*>(p->bsum);
         tr = trace_begin("batch_msm_accumulate", st);
         k_accumulate<F, LZK_BASES_AFFINE><<<grid_for(p->chunks, 128), 128, 0, st>>>(
-            p->bases, p->ent, p->off, (uint32_t)p->total_buckets, p->chunks, p->chunk, bsum, static_cast<X*>(p->head),
-            static_cast<X*>(p->tail)); note_launch();
+            p->bases, p->ent, p->off, (uint32_t)p->total_buckets, p->chunks, p->chunk, p->total_pts, bsum,
+            static_cast<X*>(p->head), static_cast<X*>(p->tail)); note_launch();
         trace_end(tr, st);
         tr = trace_begin("batch_msm_fixup", st);
         LZK_CUDA(cudaMemsetAsync(p->large, 0, sizeof(uint32_t), st));
-        k_fixup<F><<<grid_for(p->total_buckets, 256, sm_count() * 8), 256, 0, st>>>(p->off, (uint32_t)p->total_buckets, p->chunk, bsum,
+        k_fixup<F><<<grid_for(p->total_buckets, 256, sm_count() * 8), 256, 0, st>>>(p->off, (uint32_t)p->total_buckets, p->chunk, p->chunks, bsum,
                                                                             static_cast<X*>(p->head),
                                                                             static_cast<X*>(p->tail), p->large); note_launch();
         constexpr unsigned fx_threads = 32768 / sizeof(X);
@@ -318,6 +318,8 @@ static int create_plan(const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_des
     LZK_CUDA(cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming));
     return LZK_OK;
 }
+
+uint32_t debug_word_batch(bool clear) { return debug_word_here(clear); }
 
 }  // namespace lzk
 

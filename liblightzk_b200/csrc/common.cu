@@ -96,6 +96,21 @@ const char* lzk_status_string(int status)
     }
 }
 
+uint32_t lzk_debug_check_word(int clear)
+{
+    bool c = clear != 0;
+    return lzk::debug_word_sort(c) | lzk::debug_word_g1(c) | lzk::debug_word_g2(c) | lzk::debug_word_batch(c);
+}
+
+int lzk_debug_checks_enabled(void)
+{
+#ifdef LZK_DEBUG_CHECKS
+    return 1;
+#else
+    return 0;
+#endif
+}
+
 int lzk_debug_fail_allocations(long long after)
 {
     lzk::g_fail_after.store(after < 0 ? -1 : after);

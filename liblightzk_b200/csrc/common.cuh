@@ -95,6 +95,42 @@ struct Carver {
     template <class T> size_t take(size_t count) { size_t o = off; off = align_up(off + count * sizeof(T)); return o; }
 };
 
+// Debug builds (compiled with -DLZK_DEBUG_CHECKS, see build.py --debug):
+// kernels check the indices their inputs imply before they use them and,
+// where one is out of range, set a bit of a device error word and skip the
+// access instead of reading or writing outside their buffers.  The word is
+// read with lzk_debug_check_word().  Release builds compile the checks away
+// (LZK_CHECK is then always true and costs nothing).
+//   bit 0  a digit's bucket index beyond the bucket count (sort)
+//   bit 1  a scatter slot outside its bucket's range (sort)
+//   bit 2  a sorted entry naming a base beyond the table (accumulation)
+//   bit 3  a bucket offset read beyond the offsets array (accumulation)
+//   bit 4  a fix-up partial beyond the chunk count (fix-up)
+#ifdef LZK_DEBUG_CHECKS
+static __device__ uint32_t g_lzk_debug_word;
+#define LZK_CHECK(cond, bit) ((cond) ? true : (atomicOr(&g_lzk_debug_word, 1u << (bit)), false))
+// host side: this file's error word (cleared when clear is set)
+static inline uint32_t debug_word_here(bool clear)
+{
+    uint32_t v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_lzk_debug_word, sizeof(v)) != cudaSuccess) { cudaGetLastError(); return 0; }
+    if (clear) {
+        uint32_t z = 0;
+        if (cudaMemcpyToSymbol(g_lzk_debug_word, &z, sizeof(z)) != cudaSuccess) cudaGetLastError();
+    }
+    return v;
+}
+#else
+#define LZK_CHECK(cond, bit) true
+static inline uint32_t debug_word_here(bool) { return 0; }
+#endif
+// the error words of the files whose kernels check (msm_sort.cu, msm_g1.cu,
+// msm_g2.cu, batch.cu)
+uint32_t debug_word_sort(bool clear);
+uint32_t debug_word_g1(bool clear);
+uint32_t debug_word_g2(bool clear);
+uint32_t debug_word_batch(bool clear);
+
 __device__ __forceinline__ uint64_t gtid() { return (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; }
 __device__ __forceinline__ uint64_t gstride() { return (uint64_t)gridDim.x * blockDim.x; }
 

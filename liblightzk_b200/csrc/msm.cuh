@@ -167,9 +167,10 @@ __device__ __forceinline__ Aff<F> load_base(const void* bases, uint32_t v)
 template <class F, int LAYOUT>
 __global__ void __launch_bounds__(128, sizeof(F) == 32 ? 5 : 3) k_accumulate(const void* __restrict__ bases, const uint32_t* __restrict__ ent,
                                                     const uint32_t* __restrict__ off, uint32_t B, size_t chunks,
-                                                    uint32_t chunk, XYZZ<F>* __restrict__ bsum,
+                                                    uint32_t chunk, uint64_t nbases, XYZZ<F>* __restrict__ bsum,
                                                     XYZZ<F>* __restrict__ head, XYZZ<F>* __restrict__ tail)
 {
+    (void)nbases;   // the base records behind the entries (debug checks)
     uint64_t t = gtid();
     if (t >= chunks) return;
     uint32_t T = off[B];
@@ -188,6 +189,7 @@ __global__ void __launch_bounds__(128, sizeof(F) == 32 ? 5 : 3) k_accumulate(con
             // search of 16 dependent loads, which measured 0.9 % (G1) and
             // 1.3 % (G2) faster; searched only past an empty bucket.  Since
             // e < off[B], b + 1 < B and off[b + 2] exists.
+            if (!LZK_CHECK(b + 2 <= B, 3)) return;
             bbeg = bend;
             bend = off[b + 2];
             b = b + 1;
@@ -197,7 +199,9 @@ __global__ void __launch_bounds__(128, sizeof(F) == 32 ? 5 : 3) k_accumulate(con
             }
             acc = xyzz_inf<F>();
         }
-        acc = xyzz_madd(acc, load_base<F, LAYOUT>(bases, ent[e]));
+        const uint32_t v = ent[e];
+        if (!LZK_CHECK((v & 0x7fffffffu) < nbases, 2)) continue;
+        acc = xyzz_madd(acc, load_base<F, LAYOUT>(bases, v));
     }
     bool began_before = bbeg < cs, cont_after = bend > ce;
     if (began_before) st_elem(head + t, acc);
@@ -206,13 +210,16 @@ __global__ void __launch_bounds__(128, sizeof(F) == 32 ? 5 : 3) k_accumulate(con
 }
 
 template <class F>
-__global__ void k_fixup(const uint32_t* __restrict__ off, uint32_t B, uint32_t chunk, XYZZ<F>* __restrict__ bsum,
-                        const XYZZ<F>* __restrict__ head, const XYZZ<F>* __restrict__ tail, uint32_t* __restrict__ large)
+__global__ void k_fixup(const uint32_t* __restrict__ off, uint32_t B, uint32_t chunk, uint64_t chunks,
+                        XYZZ<F>* __restrict__ bsum, const XYZZ<F>* __restrict__ head, const XYZZ<F>* __restrict__ tail,
+                        uint32_t* __restrict__ large)
 {
+    (void)chunks;
     for (uint64_t b = gtid(); b < B; b += gstride()) {
         uint32_t s = off[b], e = off[b + 1];
         if (s == e) continue;
         uint32_t c0 = s / chunk, c1 = (e - 1) / chunk;
+        if (!LZK_CHECK(c1 < chunks, 4)) continue;
         if (c0 == c1) continue;
         if (c1 - c0 > kFixSmall) {
             large[1 + atomicAdd(large, 1u)] = (uint32_t)b;
@@ -526,17 +533,19 @@ int run_msm(const Fr* scalars, const void* bases, size_t n, Jac<typename Gp::F>*
     void* tr = trace_begin(sizeof(F) == 32 ? "msm_g1_accumulate" : "msm_g2_accumulate", st);
     {
         unsigned g = grid_for(p.chunks, 128);
+        // base records the entries may name: the whole table, or the n bases
+        const uint64_t nbases = shared ? (uint64_t)cfg->precomp_windows * stride : (uint64_t)n;
         constexpr int REF = sizeof(F) == 32 ? (int)LZK_BASES_REF_G1_JAC : (int)LZK_BASES_REF_G2_LANES;
         if (layout == LZK_BASES_AFFINE) {
-            k_accumulate<F, LZK_BASES_AFFINE><<<g, 128, 0, st>>>(bases, ent, off, p.B, p.chunks, p.chunk, bsum, head, tail); note_launch();
+            k_accumulate<F, LZK_BASES_AFFINE><<<g, 128, 0, st>>>(bases, ent, off, p.B, p.chunks, p.chunk, nbases, bsum, head, tail); note_launch();
         } else {
-            k_accumulate<F, REF><<<g, 128, 0, st>>>(bases, ent, off, p.B, p.chunks, p.chunk, bsum, head, tail); note_launch();
+            k_accumulate<F, REF><<<g, 128, 0, st>>>(bases, ent, off, p.B, p.chunks, p.chunk, nbases, bsum, head, tail); note_launch();
         }
     }
     trace_end(tr, st);
     void* tr_fix = trace_begin(sizeof(F) == 32 ? "msm_g1_fixup" : "msm_g2_fixup", st);
     LZK_CUDA(cudaMemsetAsync(large, 0, sizeof(uint32_t), st));
-    k_fixup<F><<<grid_for(p.B, 256, sm_count() * 8), 256, 0, st>>>(off, p.B, p.chunk, bsum, head, tail, large); note_launch();
+    k_fixup<F><<<grid_for(p.B, 256, sm_count() * 8), 256, 0, st>>>(off, p.B, p.chunk, p.chunks, bsum, head, tail, large); note_launch();
     {
         constexpr unsigned fx_threads = 32768 / sizeof(X);   // 32 KB of shared memory
         k_fixup_large<F><<<sm_count() * 2, fx_threads, fx_threads * sizeof(X), st>>>(off, p.chunk, bsum, head, tail, large); note_launch();

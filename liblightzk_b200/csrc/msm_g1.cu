@@ -5,6 +5,8 @@
 using namespace lzk;
 
 namespace lzk {
+uint32_t debug_word_g1(bool clear) { return debug_word_here(clear); }
+
 int msm_g1_presorted(const Fr* scalars, const void* table, size_t n, Jac<Fq>* out, const lzk_msm_cfg* cfg,
                      cudaStream_t st, const uint32_t* off, const uint32_t* ent)
 {

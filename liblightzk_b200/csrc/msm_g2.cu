@@ -5,6 +5,8 @@
 using namespace lzk;
 
 namespace lzk {
+uint32_t debug_word_g2(bool clear) { return debug_word_here(clear); }
+
 int msm_g2_presorted(const Fr* scalars, const void* table, size_t n, Jac<Fq2>* out, const lzk_msm_cfg* cfg,
                      cudaStream_t st, const uint32_t* off, const uint32_t* ent)
 {

@@ -74,11 +74,14 @@ __device__ __forceinline__ const Fr* scalar_at(const Fr* lo, const Fr* hi, size_
 __global__ void k_count(const Fr* __restrict__ scalars, const Fr* __restrict__ hi, size_t split, size_t n, uint32_t c,
                         uint32_t W, uint32_t nb, bool shared, uint32_t* __restrict__ cnt)
 {
+    const uint32_t B = shared ? nb : W * nb;
+    (void)B;
     for (uint64_t i = gtid(); i < n; i += gstride()) {
         DigitIter it; it.load(scalar_at(scalars, hi, split, i));
         for (uint32_t w = 0; w < W; w++) {
             bool neg; uint32_t d = it.next(w, c, neg);
-            if (d) atomicAdd(cnt + (shared ? 0u : w * nb) + d - 1, 1u);
+            uint32_t b = (shared ? 0u : w * nb) + d - 1;
+            if (d && LZK_CHECK(b < B, 0)) atomicAdd(cnt + b, 1u);
         }
     }
 }
@@ -87,13 +90,17 @@ __global__ void k_scatter(const Fr* __restrict__ scalars, const Fr* __restrict__
                           uint32_t c, uint32_t W, uint32_t nb, bool shared, size_t stride,
                           const uint32_t* __restrict__ off, uint32_t* __restrict__ cnt, uint32_t* __restrict__ ent)
 {
+    const uint32_t B = shared ? nb : W * nb;
+    (void)B;
     for (uint64_t i = gtid(); i < n; i += gstride()) {
         DigitIter it; it.load(scalar_at(scalars, hi, split, i));
         for (uint32_t w = 0; w < W; w++) {
             bool neg; uint32_t d = it.next(w, c, neg);
             if (!d) continue;
             uint32_t b = (shared ? 0u : w * nb) + d - 1;
+            if (!LZK_CHECK(b < B, 0)) continue;
             uint32_t slot = off[b] + atomicSub(cnt + b, 1u) - 1u;
+            if (!LZK_CHECK(slot >= off[b] && slot < off[b + 1], 1)) continue;
             uint32_t idx = (uint32_t)(shared ? (size_t)w * stride + i : i);
             ent[slot] = idx | (neg ? 0x80000000u : 0u);
         }
@@ -229,6 +236,8 @@ int msm_sort_scalars(const Fr* scalars, size_t n, uint32_t c, size_t stride, uin
     trace_end(tr, st);
     return rc;
 }
+
+uint32_t debug_word_sort(bool clear) { return debug_word_here(clear); }
 
 }  // namespace lzk
 
