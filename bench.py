@@ -288,10 +288,12 @@ def run_batch_case(args):
     table_src = None if args.retune else autotune.load_default()
     if table_src is None:
         autotune.tune_msm(1, log_ns=range(10, 21), spread=2, reps=2)
+        autotune.tune_msm_table(1, log_ns=range(10, 21), reps=2)
         autotune.tune_ntt(range(12, 23), reps=2)
         table_src = "measured in this run"
     msms, ntts, _pool = batch.workload_config3()
     plan = batch.BatchPlan(1, msms, ntts)
+    plan_fx = batch.BatchPlan(1, msms, ntts, fixed_bases=True)
     stream = torch.cuda.Stream()
     torch.cuda.synchronize()
 
@@ -307,8 +309,10 @@ def run_batch_case(args):
         return out
 
     plan.run(use_graph=True, stream=stream)
+    plan_fx.run(use_graph=True, stream=stream)
     torch.cuda.synchronize()
     plan_ms = timed(lambda: plan.run(use_graph=True, stream=stream), args.reps)
+    plan_fx_ms = timed(lambda: plan_fx.run(use_graph=True, stream=stream), args.reps)
 
     def one_by_one():
         for s, b, o in msms:
@@ -318,23 +322,52 @@ def run_batch_case(args):
 
     one_by_one()
     seq_ms = timed(one_by_one, args.reps)
-    # per-phase device times of one eager (uncaptured) run of the plan
+    # one at a time over shifted-copy tables too (built outside the timing,
+    # at the width the tuning table gives tables)
+    tabs = []
+    for s, b, o in msms:
+        n = int(s.shape[0])
+        c = msm.autotune_window(1, n, precomputed=True)
+        w = msm.windows_for(c)
+        tabs.append((s, msm.precompute(1, b, c, w, n), c, w, n, o))
+
+    def one_by_one_tables():
+        for s, t, c, w, n, o in tabs:
+            msm.msm_precomputed(1, s, t, c, w, n, out=o, stream=stream)
+        for d, k, di in ntts:
+            ntt.ntt(d, k, di, stream=stream)
+
+    one_by_one_tables()
+    seq_tab_ms = timed(one_by_one_tables, args.reps)
+    del tabs
+    # per-phase device times of one eager (uncaptured) run of each plan
     from liblightzk_b200 import _capi
-    _capi.trace_reset()
-    _capi.trace_enable(True)
-    plan.run(use_graph=False, stream=stream)
-    torch.cuda.synchronize()
-    _capi.trace_enable(False)
-    phases = {ph: _capi.trace_get(f"batch_{ph}")[0] for ph in ("msm_sort", "msm_accumulate", "msm_fixup",
-                                                                "msm_reduce", "msm_finish", "ntt")}
+
+    def phases_of(pl):
+        _capi.trace_reset()
+        _capi.trace_enable(True)
+        pl.run(use_graph=False, stream=stream)
+        torch.cuda.synchronize()
+        _capi.trace_enable(False)
+        return {ph: _capi.trace_get(f"batch_{ph}")[0] for ph in ("msm_sort", "msm_accumulate", "msm_fixup",
+                                                                  "msm_reduce", "msm_finish", "ntt")}
+
+    phases, phases_fx = phases_of(plan), phases_of(plan_fx)
     pts = sum(int(m[0].shape[0]) for m in msms)
     elems = sum(1 << k for _, k, _ in ntts)
+    med = lambda x: float(np.median(x))  # noqa: E731
     print(json.dumps({"case": "batch", "msms": len(msms), "ntts": len(ntts), "msm_points": pts,
-                      "ntt_elements": elems, "plan_graph_ms": plan_ms, "one_by_one_ms": seq_ms,
-                      "speedup": float(np.median(seq_ms) / np.median(plan_ms)),
-                      "plan_device_bytes": plan.device_bytes(), "phases_ms_eager": phases,
+                      "ntt_elements": elems,
+                      "plan_fixed_bases_graph_ms": plan_fx_ms, "plan_graph_ms": plan_ms,
+                      "one_by_one_ms": seq_ms, "one_by_one_tables_ms": seq_tab_ms,
+                      "speedup": med(seq_ms) / med(plan_fx_ms),
+                      "speedup_vs_one_by_one_tables": med(seq_tab_ms) / med(plan_fx_ms),
+                      "speedup_plain_plan": med(seq_ms) / med(plan_ms),
+                      "plan_device_bytes": plan.device_bytes(), "plan_fixed_bases_device_bytes": plan_fx.device_bytes(),
+                      "phases_ms_eager": phases, "phases_ms_eager_fixed_bases": phases_fx,
                       "tuning_table": table_src,
-                      "tuned": {"msm_g1": {lg: {k: autotune.get_value(k, 1, lg) for k in ("window", "run", "chunk")}
+                      "tuned": {"msm_g1": {lg: {k: autotune.get_value(k, 1, lg)
+                                                for k in ("window", "table_window", "run", "chunk")}
                                            for lg in range(10, 21)},
                                 "ntt_block": {lg: autotune.get_value("ntt", 0, lg) for lg in range(12, 23)}}}),
           flush=True)
@@ -446,6 +479,7 @@ def run_tune_case(args):
     t0 = time.time()
     t1 = autotune.tune_msm(1, log_ns=range(10, 22), spread=2, reps=2)
     t2 = autotune.tune_msm(2, log_ns=range(10, 21), spread=1, reps=2)
+    tt = autotune.tune_msm_table(1, log_ns=range(10, 21), reps=2)
     tn = autotune.tune_ntt(range(10, 25), reps=2)
     circ = synth.Circuit(args.log_m, seed=1)
     pk = synth.ProvingKey(circ, seed=7)
@@ -455,6 +489,7 @@ def run_tune_case(args):
     print(json.dumps({"case": "tune", "seconds": time.time() - t0,
                       "msm_g1": {lg: {k: v[k] for k in ("window", "run", "chunk")} for lg, v in t1.items()},
                       "msm_g2": {lg: {k: v[k] for k in ("window", "run", "chunk")} for lg, v in t2.items()},
+                      "msm_g1_table_window": {lg: {"best": v[0], "ms": v[1]} for lg, v in tt.items()},
                       "ntt_block": {lg: {"best": v[0], "ms": v[1]} for lg, v in tn.items()},
                       "prover_ms_per_proof": {f"chunk {c}, run {r}": ms for (c, r), ms in tp.items()}}), flush=True)
 

@@ -426,6 +426,16 @@ typedef struct lzk_batch_plan lzk_batch_plan;
 
 int lzk_batch_plan_create(int group, const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_desc* ntts, size_t n_ntt,
                           lzk_batch_plan** out);
+/* The same with flags.  LZK_BATCH_FIXED_BASES: the MSMs' bases are read once,
+ * at creation, into shifted-copy tables (as lzk_g1_precompute builds; the
+ * plan then holds sum_k n_k * ceil(255 / c_k) points), so every window of an
+ * MSM shares one bucket set and no window combination remains; later
+ * changes to the bases arrays are not seen (the scalars are still read at
+ * every run).  For bases that stay fixed, such as a proving key's queries.
+ * Window widths come from LZK_TUNE_MSM_TABLE_WINDOW. */
+#define LZK_BATCH_FIXED_BASES 0x1u
+int lzk_batch_plan_create_ex(int group, const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_desc* ntts,
+                             size_t n_ntt, uint32_t flags, lzk_batch_plan** out);
 int lzk_batch_plan_run(lzk_batch_plan* plan, int use_graph, void* stream);
 size_t lzk_batch_plan_device_bytes(const lzk_batch_plan* plan);
 int lzk_batch_plan_destroy(lzk_batch_plan* plan);
@@ -442,6 +452,9 @@ int lzk_batch_plan_destroy(lzk_batch_plan* plan);
  *   LZK_TUNE_NTT_BLOCK       elements per block of an NTT pass (the stages
  *                            a pass runs in shared memory), 256..4096, power
  *                            of two; unset: 2048
+ *   LZK_TUNE_MSM_TABLE_WINDOW window width of MSMs over shifted-copy tables
+ *                            that leave it open (batch plans with
+ *                            LZK_BATCH_FIXED_BASES); unset: the cost model
  * The reference fixes all of these at compile time (c = 12 with 4096
  * buckets, msm.cuh:216-227; one launch per NTT stage, poly.cuh:42-63).
  * value 0 clears an entry.  A Groth16 prover and a batch plan read the table
@@ -451,6 +464,7 @@ int lzk_batch_plan_destroy(lzk_batch_plan* plan);
 #define LZK_TUNE_MSM_CHUNK      1
 #define LZK_TUNE_MSM_REDUCE_RUN 2
 #define LZK_TUNE_NTT_BLOCK      3
+#define LZK_TUNE_MSM_TABLE_WINDOW 4
 int lzk_tune_set(int knob, int group, uint32_t log_n, uint32_t value);
 /* The value in effect (the entry, or the default; 0 for an unset window). */
 uint32_t lzk_tune_get(int knob, int group, uint32_t log_n);

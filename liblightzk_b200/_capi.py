@@ -61,6 +61,7 @@ SIGNATURES = {
     "lzk_server_reset_stats": (c_i, [c_p]),
     "lzk_server_destroy": (c_i, [c_p]),
     "lzk_batch_plan_create": (c_i, [c_i, c_p, c_sz, c_p, c_sz, c_p]),
+    "lzk_batch_plan_create_ex": (c_i, [c_i, c_p, c_sz, c_p, c_sz, c_u32, c_p]),
     "lzk_batch_plan_run": (c_i, [c_p, c_i, c_p]),
     "lzk_batch_plan_device_bytes": (c_sz, [c_p]),
     "lzk_batch_plan_destroy": (c_i, [c_p]),

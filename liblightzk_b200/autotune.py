@@ -9,6 +9,8 @@ seeded random inputs, median of a few runs) and installs the fastest:
   run     buckets per lane run in the bucket-reduction tiles (4, 8, 16)
   ntt     elements per block of an NTT pass, i.e. how a transform's stages
           split into passes (1024, 2048, 4096)
+  table_window  window width of MSMs over shifted-copy tables (batch plans
+          with fixed bases)
 
 Every autotuned MSM, batch plan and prover made afterwards uses the table
 (a prover or plan reads it when it is created).  `save` / `load` keep a
@@ -25,8 +27,8 @@ from . import _capi, msm, ntt, synth
 # measured tables shipped with the package, by GPU name
 DEFAULT_TABLES = {"B200": os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning", "b200.json")}
 
-WINDOW, CHUNK, RUN, NTT_BLOCK = 0, 1, 2, 3
-KNOBS = {"window": WINDOW, "chunk": CHUNK, "run": RUN, "ntt": NTT_BLOCK}
+WINDOW, CHUNK, RUN, NTT_BLOCK, TABLE_WINDOW = 0, 1, 2, 3, 4
+KNOBS = {"window": WINDOW, "chunk": CHUNK, "run": RUN, "ntt": NTT_BLOCK, "table_window": TABLE_WINDOW}
 
 
 def _time(fn, reps):
@@ -104,6 +106,28 @@ def tune_msm(group=1, log_ns=range(10, 21), spread=2, reps=3, seed=11, chunks=(3
     return out
 
 
+def tune_msm_table(group=1, log_ns=range(10, 21), widths=range(11, 19), reps=3, seed=11):
+    """window width of MSMs over shifted-copy tables (batch plans with fixed
+    bases) per size class; installs the fastest and returns
+    {log_n: (best_c, {c: ms})}"""
+    out = {}
+    top = max(log_ns)
+    sc_all = synth.random_fr(1 << top, seed, 90)
+    bases_all = synth.fixed_base(group, synth.random_fr(1 << top, seed, 91))
+    for lg in log_ns:
+        n = 1 << lg
+        res = {}
+        for c in widths:
+            w = msm.windows_for(c)
+            t = msm.precompute(group, bases_all[:n], c, w, n)
+            res[c] = _time(lambda: msm.msm_precomputed(group, sc_all[:n], t, c, w, n), reps)
+            del t
+        best = min(res, key=res.get)
+        set_value("table_window", group, lg, best)
+        out[lg] = (best, res)
+    return out
+
+
 def tune_ntt(log_ns=range(12, 23), reps=3, seed=12, blocks=(1024, 2048, 4096), direction=ntt.COSET_FORWARD):
     """NTT block size per transform size; installs the fastest and returns
     {log_n: (best, {block: ms})}"""
@@ -166,7 +190,8 @@ def current(groups=(1, 2), log_ns=range(0, 33)):
     """the installed table as a JSON-able dict of non-default entries"""
     t = {"msm": {}, "ntt": {}}
     for g in groups:
-        t["msm"][str(g)] = {k: {str(lg): get_value(k, g, lg) for lg in log_ns} for k in ("window", "chunk", "run")}
+        t["msm"][str(g)] = {k: {str(lg): get_value(k, g, lg) for lg in log_ns}
+                            for k in ("window", "chunk", "run", "table_window")}
     t["ntt"] = {str(lg): get_value("ntt", 0, lg) for lg in log_ns}
     return t
 

@@ -16,8 +16,13 @@ from . import _capi
 from .device import ptr, stream_ptr
 
 
+FIXED_BASES = 0x1
+
+
 class BatchPlan:
-    def __init__(self, group, msms=(), ntts=()):
+    def __init__(self, group, msms=(), ntts=(), fixed_bases=False):
+        """fixed_bases: build the MSMs' shifted-copy tables now (the bases are
+        not read again; see LZK_BATCH_FIXED_BASES)"""
         self.group = group
         self._keep = (list(msms), list(ntts))
         md = (_capi.MsmDesc * max(len(msms), 1))()
@@ -29,8 +34,8 @@ class BatchPlan:
         for i, (d, k, direction) in enumerate(ntts):
             nd[i].data, nd[i].log_n, nd[i].direction = ptr(d), k, direction
         h = ctypes.c_void_p()
-        _capi.call("lzk_batch_plan_create", group, md if msms else None, len(msms), nd if ntts else None, len(ntts),
-                   ctypes.byref(h))
+        _capi.call("lzk_batch_plan_create_ex", group, md if msms else None, len(msms), nd if ntts else None,
+                   len(ntts), FIXED_BASES if fixed_bases else 0, ctypes.byref(h))
         self.handle = h
 
     def run(self, use_graph=False, stream=None):

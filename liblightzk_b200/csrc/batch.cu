@@ -26,13 +26,20 @@ struct BDesc {                 // per MSM, device side
     uint64_t pts_off;          // first point in the gathered base array
     uint64_t n;
     uint64_t bucket_base;      // first bucket in the global bucket space
-    uint64_t win_base;         // first window in the window-result array
+    uint64_t win_base;         // first window result in the window-result array
     void* out;
-    uint32_t c, W, nb, pad;
+    uint64_t tab_off;          // fixed bases: first entry of this MSM's shifted-copy table
+    uint32_t c, W, nb;
+    uint32_t hw;               // window results the finish combines: W (plain bases) or 1 (table)
 };
 
 struct lzk_batch_plan {
     int group = 1;
+    uint32_t flags = 0;                // LZK_BATCH_*
+    bool fixed = false;                // LZK_BATCH_FIXED_BASES: shifted-copy tables built at creation
+    void* table = nullptr;             // their entries, all MSMs, table_pts points
+    uint64_t table_pts = 0;
+    size_t table_bytes = 0;
     std::vector<BDesc> msm;            // sorted by window width
     struct WGroup { uint32_t c; uint64_t bucket_base, windows; };
     std::vector<WGroup> wgroups;
@@ -85,9 +92,13 @@ __device__ __forceinline__ uint32_t bwindow_bits(const uint32_t s[8], uint32_t l
     return (uint32_t)v & ((1u << c) - 1u);
 }
 
+// With tables (shared = true) every window of an MSM lands in its one
+// bucket set and an entry names the table copy of its window:
+// tab_off + w n + i; with plain bases each window has its own set and an
+// entry names the gathered base i.
 template <bool SCATTER>
 __global__ void k_bdigits(const BDesc* __restrict__ d, const uint64_t* __restrict__ ptsoff, uint32_t count,
-                          uint64_t total, const uint32_t* __restrict__ off, uint32_t* __restrict__ cnt,
+                          uint64_t total, bool shared, const uint32_t* __restrict__ off, uint32_t* __restrict__ cnt,
                           uint32_t* __restrict__ ent)
 {
     for (uint64_t i = gtid(); i < total; i += gstride()) {
@@ -102,10 +113,11 @@ __global__ void k_bdigits(const BDesc* __restrict__ d, const uint64_t* __restric
             if (raw > half) { carry = 1; neg = true; a = (1u << m.c) - raw; }
             else { carry = 0; neg = false; a = raw; }
             if (!a) continue;
-            uint32_t b = (uint32_t)(m.bucket_base + (uint64_t)w * m.nb + a - 1);
+            uint32_t b = (uint32_t)(m.bucket_base + (shared ? 0 : (uint64_t)w * m.nb) + a - 1);
             if (SCATTER) {
                 uint32_t slot = off[b] + atomicSub(cnt + b, 1u) - 1u;
-                ent[slot] = (uint32_t)i | (neg ? 0x80000000u : 0u);
+                uint32_t idx = shared ? (uint32_t)(m.tab_off + (uint64_t)w * m.n + (i - m.pts_off)) : (uint32_t)i;
+                ent[slot] = idx | (neg ? 0x80000000u : 0u);
             } else {
                 atomicAdd(cnt + b, 1u);
             }
@@ -124,8 +136,8 @@ __global__ void k_bfinish(const BDesc* __restrict__ d, uint32_t count, const XYZ
     const BDesc& m = d[k];
     XYZZ<F> r = xyzz_inf<F>();
     if (m.n) {
-        for (int w = (int)m.W - 1; w >= 0; w--) {
-            if (w != (int)m.W - 1)
+        for (int w = (int)m.hw - 1; w >= 0; w--) {
+            if (w != (int)m.hw - 1)
                 for (uint32_t b = 0; b < m.c; b++) r = xyzz_dbl_warp(r);
             r = xyzz_add_warp(r, ld_elem(wres + m.win_base + w));
         }
@@ -142,17 +154,19 @@ static int run_plan(lzk_batch_plan* p, cudaStream_t st)
     if (count && p->total_pts) {
         unsigned g = grid_for(p->total_pts, 256, sm_count() * 16);
         void* tr = trace_begin("batch_msm_sort", st);
-        k_bgather<F><<<g, 256, 0, st>>>(p->d_desc, p->d_ptsoff, count, p->total_pts, static_cast<Aff<F>*>(p->bases)); note_launch();
+        if (!p->fixed) {
+            k_bgather<F><<<g, 256, 0, st>>>(p->d_desc, p->d_ptsoff, count, p->total_pts, static_cast<Aff<F>*>(p->bases)); note_launch();
+        }
         LZK_CUDA(cudaMemsetAsync(p->cnt, 0, sizeof(uint32_t) * p->total_buckets, st));
-        k_bdigits<false><<<g, 256, 0, st>>>(p->d_desc, p->d_ptsoff, count, p->total_pts, p->off, p->cnt, p->ent); note_launch();
+        k_bdigits<false><<<g, 256, 0, st>>>(p->d_desc, p->d_ptsoff, count, p->total_pts, p->fixed, p->off, p->cnt, p->ent); note_launch();
         LZK_TRY(scan_offsets(p->cnt, (uint32_t)p->total_buckets, p->off, p->bsums, st));
-        k_bdigits<true><<<g, 256, 0, st>>>(p->d_desc, p->d_ptsoff, count, p->total_pts, p->off, p->cnt, p->ent); note_launch();
+        k_bdigits<true><<<g, 256, 0, st>>>(p->d_desc, p->d_ptsoff, count, p->total_pts, p->fixed, p->off, p->cnt, p->ent); note_launch();
         trace_end(tr, st);
         X* bsum = static_cast<X*>(p->bsum);
         tr = trace_begin("batch_msm_accumulate", st);
         k_accumulate<F, LZK_BASES_AFFINE><<<grid_for(p->chunks, 128), 128, 0, st>>>(
-            p->bases, p->ent, p->off, (uint32_t)p->total_buckets, p->chunks, p->chunk, p->total_pts, bsum,
-            static_cast<X*>(p->head), static_cast<X*>(p->tail)); note_launch();
+            p->fixed ? p->table : p->bases, p->ent, p->off, (uint32_t)p->total_buckets, p->chunks, p->chunk,
+            p->fixed ? p->table_pts : p->total_pts, bsum, static_cast<X*>(p->head), static_cast<X*>(p->tail)); note_launch();
         trace_end(tr, st);
         tr = trace_begin("batch_msm_fixup", st);
         LZK_CUDA(cudaMemsetAsync(p->large, 0, sizeof(uint32_t), st));
@@ -204,6 +218,7 @@ static void destroy_plan(lzk_batch_plan* p)
     if (p->exec) cudaGraphExecDestroy(p->exec);
     if (p->graph) cudaGraphDestroy(p->graph);
     if (p->ws) cudaFree(p->ws);
+    if (p->table) cudaFree(p->table);
     for (auto& g : p->ngroups) if (g.ptrs) cudaFree(g.ptrs);
     if (p->s_ntt) cudaStreamDestroy(p->s_ntt);
     if (p->ev_fork) cudaEventDestroy(p->ev_fork);
@@ -221,7 +236,7 @@ static int create_plan(const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_des
     std::vector<uint32_t> cw(n_msm);
     for (size_t i = 0; i < n_msm; i++) {
         if (!msms[i].out || (msms[i].n && (!msms[i].scalars || !msms[i].bases))) return LZK_EINVAL;
-        cw[i] = msms[i].window_bits ? msms[i].window_bits : msm_autotune(p->group, msms[i].n, false);
+        cw[i] = msms[i].window_bits ? msms[i].window_bits : msm_autotune(p->group, msms[i].n, p->fixed);
         if (cw[i] < 2 || cw[i] > 24) return LZK_EINVAL;
         order[i] = i;
     }
@@ -240,16 +255,22 @@ static int create_plan(const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_des
         d.pts_off = p->total_pts;
         d.bucket_base = p->total_buckets;
         d.win_base = p->total_windows;
+        // plain bases: a bucket set per window, combined by Horner; tables:
+        // one set for all windows
+        d.hw = p->fixed ? 1 : d.W;
+        d.tab_off = p->table_pts;
+        if (p->fixed) p->table_pts += m.n * (uint64_t)d.W;
         p->total_pts += m.n;
-        p->total_buckets += (uint64_t)d.W * d.nb;
-        p->total_windows += d.W;
+        p->total_buckets += (uint64_t)d.hw * d.nb;
+        p->total_windows += d.hw;
         p->max_entries += m.n * (uint64_t)d.W;
         if (p->wgroups.empty() || p->wgroups.back().c != d.c) p->wgroups.push_back({d.c, d.bucket_base, 0});
-        p->wgroups.back().windows += d.W;
+        p->wgroups.back().windows += d.hw;
         ptsoff.push_back(d.pts_off);
         p->msm.push_back(d);
     }
-    if (p->total_pts >= (1ull << 31) || p->total_buckets >= (1ull << 32) - 1 || p->max_entries >= (1ull << 32))
+    if (p->total_pts >= (1ull << 31) || p->table_pts >= (1ull << 31) || p->total_buckets >= (1ull << 32) - 1 ||
+        p->max_entries >= (1ull << 32))
         return LZK_EINVAL;
     // the plan's largest MSM picks the accumulation chunk and reduction run
     size_t largest = 0;
@@ -269,7 +290,7 @@ static int create_plan(const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_des
     size_t o_bsums = cv.take<uint32_t>((B + 4095) / 4096 + 1);
     size_t o_large = cv.take<uint32_t>(p->chunks / kFixSmall + 2);
     size_t o_ent = cv.take<uint32_t>(std::max<uint64_t>(p->max_entries, 1));
-    size_t o_bases = cv.take<Aff<F>>(std::max<uint64_t>(p->total_pts, 1));
+    size_t o_bases = cv.take<Aff<F>>(p->fixed ? 1 : std::max<uint64_t>(p->total_pts, 1));
     size_t o_bsum = cv.take<X>(B);
     size_t o_head = cv.take<X>(std::max<uint64_t>(p->chunks, 1)), o_tail = cv.take<X>(std::max<uint64_t>(p->chunks, 1));
     size_t o_lr0 = cv.take<X>(std::max<uint64_t>(p->lvl, 1)), o_lr1 = cv.take<X>(std::max<uint64_t>(p->lvl, 1));
@@ -294,6 +315,22 @@ static int create_plan(const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_des
     if (n_msm) {
         LZK_CUDA(cudaMemcpy(p->d_desc, p->msm.data(), sizeof(BDesc) * n_msm, cudaMemcpyHostToDevice));
         LZK_CUDA(cudaMemcpy(p->d_ptsoff, ptsoff.data(), sizeof(uint64_t) * n_msm, cudaMemcpyHostToDevice));
+    }
+    if (p->fixed && p->table_pts) {
+        // the shifted-copy table of every MSM, entry (w, i) at tab_off + w n + i
+        p->table_bytes = p->table_pts * sizeof(Aff<F>);
+        LZK_TRY(dev_malloc(&p->table, p->table_bytes));
+        cudaStream_t st;
+        LZK_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        int rc = LZK_OK;
+        for (const BDesc& d : p->msm) {
+            if (!d.n || rc != LZK_OK) continue;
+            rc = run_precompute<F>(static_cast<const Aff<F>*>(d.bases), d.n, d.c, d.W,
+                                   static_cast<Aff<F>*>(p->table) + d.tab_off, d.n, st);
+        }
+        if (rc == LZK_OK) rc = cuda_status(cudaStreamSynchronize(st));
+        cudaStreamDestroy(st);
+        LZK_TRY(rc);
     }
     // NTTs: groups of equal (size, direction) with a device pointer table each
     std::map<std::pair<uint32_t, int>, std::vector<Fr*>> groups;
@@ -327,18 +364,27 @@ using namespace lzk;
 
 extern "C" {
 
-int lzk_batch_plan_create(int group, const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_desc* ntts, size_t n_ntt,
-                          lzk_batch_plan** out)
+int lzk_batch_plan_create_ex(int group, const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_desc* ntts,
+                             size_t n_ntt, uint32_t flags, lzk_batch_plan** out)
 {
     if (!out || (group != 1 && group != 2) || (n_msm && !msms) || (n_ntt && !ntts)) return LZK_EINVAL;
+    if (flags & ~LZK_BATCH_FIXED_BASES) return LZK_EINVAL;
     *out = nullptr;
     lzk_batch_plan* p = new (std::nothrow) lzk_batch_plan();
     if (!p) return LZK_ENOMEM;
     p->group = group;
+    p->flags = flags;
+    p->fixed = (flags & LZK_BATCH_FIXED_BASES) != 0;
     int rc = group == 2 ? create_plan<Fq2>(msms, n_msm, ntts, n_ntt, p) : create_plan<Fq>(msms, n_msm, ntts, n_ntt, p);
     if (rc != LZK_OK) { destroy_plan(p); return rc; }
     *out = p;
     return LZK_OK;
+}
+
+int lzk_batch_plan_create(int group, const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_desc* ntts, size_t n_ntt,
+                          lzk_batch_plan** out)
+{
+    return lzk_batch_plan_create_ex(group, msms, n_msm, ntts, n_ntt, 0, out);
 }
 
 int lzk_batch_plan_run(lzk_batch_plan* p, int use_graph, void* stream)
@@ -364,7 +410,7 @@ int lzk_batch_plan_run(lzk_batch_plan* p, int use_graph, void* stream)
     return LZK_OK;
 }
 
-size_t lzk_batch_plan_device_bytes(const lzk_batch_plan* p) { return p ? p->ws_bytes : 0; }
+size_t lzk_batch_plan_device_bytes(const lzk_batch_plan* p) { return p ? p->ws_bytes + p->table_bytes : 0; }
 
 int lzk_batch_plan_destroy(lzk_batch_plan* p)
 {

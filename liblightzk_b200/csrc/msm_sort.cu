@@ -200,8 +200,8 @@ int msm_sort(const MsmPlan& p, const Fr* scalars, uint32_t* cnt, uint32_t* off, 
 // ceil(log2 n); an unset entry falls back to the model
 uint32_t msm_autotune(int group, size_t n, bool shared)
 {
-    if (!shared && n && group >= 1 && group <= 2) {
-        uint32_t w = tune_lookup(LZK_TUNE_MSM_WINDOW, group, n);
+    if (n && group >= 1 && group <= 2) {
+        uint32_t w = tune_lookup(shared ? LZK_TUNE_MSM_TABLE_WINDOW : LZK_TUNE_MSM_WINDOW, group, n);
         if (w) return w;
     }
     (void)group;

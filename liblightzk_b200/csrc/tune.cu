@@ -54,7 +54,8 @@ bool tune_valid(int knob, uint32_t v)
 {
     if (v == 0) return true;
     switch (knob) {
-        case LZK_TUNE_MSM_WINDOW: return v >= 2 && v <= 24;
+        case LZK_TUNE_MSM_WINDOW:
+        case LZK_TUNE_MSM_TABLE_WINDOW: return v >= 2 && v <= 24;
         case LZK_TUNE_MSM_CHUNK: return pow2(v) && v >= kMinChunk && v <= kMaxChunk;
         case LZK_TUNE_MSM_REDUCE_RUN: return pow2(v) && v <= kMaxRun;
         case LZK_TUNE_NTT_BLOCK: return pow2(v) && v >= kMinNttBlock && v <= kMaxNttBlock;

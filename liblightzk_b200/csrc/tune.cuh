@@ -6,7 +6,7 @@
 
 namespace lzk {
 
-constexpr int kTuneKnobs = 4;
+constexpr int kTuneKnobs = 5;
 constexpr uint32_t kDefaultChunk = 64, kMinChunk = 8, kMaxChunk = 512;
 constexpr uint32_t kDefaultRun = 4, kMaxRun = 16;
 constexpr uint32_t kDefaultNttBlock = 2048, kMinNttBlock = 256, kMaxNttBlock = 4096;

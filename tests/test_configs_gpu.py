@@ -4,7 +4,8 @@ against the oracle.
 * Batched operators: the exact workload the bench times (64 G1 MSMs of
   2^10..2^20 points drawn log-uniformly, over slices of one pool of 2^20
   random points, and 32 Fr NTTs of 2^12..2^22 elements in all four
-  directions), run as one plan through its captured CUDA graph; every MSM
+  directions), run as one plan through its captured CUDA graph, with plain
+  bases and with shifted-copy tables built at creation; every MSM
   result equals the oracle's MSM (the reference checks its MSM the same
   way, GPU against CPU, test/msm-check.cu:45-58) and every NTT output the
   oracle's transform, element for element.
@@ -29,30 +30,31 @@ def _host(t):
 
 
 def test_batched_workload_against_oracle(cuda, orc):
+    """both plan forms: plain bases, and shifted-copy tables built at creation"""
     import torch
 
     from liblightzk_b200 import batch
     msms, ntts, pool = batch.workload_config3()
-    ntt_in = [_host(d) for d, _, _ in ntts]
-    plan = batch.BatchPlan(1, msms, ntts)
-    stream = torch.cuda.Stream()
-    plan.run(use_graph=True, stream=stream)     # captures the graph
-    torch.cuda.synchronize()
-    # replay on fresh NTT inputs (the MSM inputs are unchanged)
-    for (d, _, _), h in zip(ntts, ntt_in):
-        d.copy_(torch.from_numpy(h.view(np.int64)).to(d.device))
-    torch.cuda.synchronize()
-    plan.run(use_graph=True, stream=stream)
-    torch.cuda.synchronize()
     sizes = [int(s.shape[0]) for s, _, _ in msms]
     assert len(msms) == 64 and max(sizes) > (1 << 19) and min(sizes) >= (1 << 10)
     assert len(ntts) == 32 and max(k for _, k, _ in ntts) >= 21
-    for s, b, o in msms:
-        want = orc.msm(1, _host(s), _host(b))
-        assert same_point(orc, 1, _host(o), want), f"MSM of {s.shape[0]} points"
-    for (d, k, di), h in zip(ntts, ntt_in):
-        assert (_host(d) == orc.ntt(h, k, di)).all(), f"NTT 2^{k} direction {di}"
-    plan.close()
+    ntt_in = [_host(d) for d, _, _ in ntts]
+    want_msm = [orc.msm(1, _host(s), _host(b)) for s, b, _ in msms]
+    want_ntt = [orc.ntt(h, k, di) for (_, k, di), h in zip(ntts, ntt_in)]
+    stream = torch.cuda.Stream()
+    for fixed in (False, True):
+        plan = batch.BatchPlan(1, msms, ntts, fixed_bases=fixed)
+        for _ in range(2):        # captures the graph, then replays it on fresh NTT inputs
+            for (d, _, _), h in zip(ntts, ntt_in):
+                d.copy_(torch.from_numpy(h.view(np.int64)).to(d.device))
+            torch.cuda.synchronize()
+            plan.run(use_graph=True, stream=stream)
+            torch.cuda.synchronize()
+        for (s, b, o), want in zip(msms, want_msm):
+            assert same_point(orc, 1, _host(o), want), f"MSM of {s.shape[0]} points (fixed bases {fixed})"
+        for (d, k, di), want in zip(ntts, want_ntt):
+            assert (_host(d) == want).all(), f"NTT 2^{k} direction {di} (fixed bases {fixed})"
+        plan.close()
 
 
 def test_serving_mix_at_benchmark_sizes(cuda, orc):
