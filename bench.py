@@ -367,7 +367,8 @@ def run_batch_case(args):
                       "phases_ms_eager": phases, "phases_ms_eager_fixed_bases": phases_fx,
                       "tuning_table": table_src,
                       "tuned": {"msm_g1": {lg: {k: autotune.get_value(k, 1, lg)
-                                                for k in ("window", "table_window", "run", "chunk")}
+                                                for k in ("window", "run", "chunk", "table_window", "table_run",
+                                                          "table_chunk")}
                                            for lg in range(10, 21)},
                                 "ntt_block": {lg: autotune.get_value("ntt", 0, lg) for lg in range(12, 23)}}}),
           flush=True)
@@ -489,7 +490,7 @@ def run_tune_case(args):
     print(json.dumps({"case": "tune", "seconds": time.time() - t0,
                       "msm_g1": {lg: {k: v[k] for k in ("window", "run", "chunk")} for lg, v in t1.items()},
                       "msm_g2": {lg: {k: v[k] for k in ("window", "run", "chunk")} for lg, v in t2.items()},
-                      "msm_g1_table_window": {lg: {"best": v[0], "ms": v[1]} for lg, v in tt.items()},
+                      "msm_g1_table": {lg: {k: v[k] for k in ("window", "run", "chunk")} for lg, v in tt.items()},
                       "ntt_block": {lg: {"best": v[0], "ms": v[1]} for lg, v in tn.items()},
                       "prover_ms_per_proof": {f"chunk {c}, run {r}": ms for (c, r), ms in tp.items()}}), flush=True)
 

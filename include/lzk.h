@@ -445,16 +445,24 @@ int lzk_batch_plan_destroy(lzk_batch_plan* plan);
  * configuration leaves it open:
  *   LZK_TUNE_MSM_WINDOW      window width of plain-base MSMs (cfg
  *                            window_bits = 0); unset: the cost model
- *   LZK_TUNE_MSM_CHUNK       sorted entries per accumulation thread (cfg
- *                            acc_chunk = 0), 8..512, power of two; unset: 64
- *   LZK_TUNE_MSM_REDUCE_RUN  buckets per lane run in the reduction tiles
- *                            (cfg reduce_run = 0), 1..16; unset: 4
+ *   LZK_TUNE_MSM_CHUNK       sorted entries per accumulation thread of a
+ *                            plain-base MSM (cfg acc_chunk = 0), 8..512,
+ *                            power of two; unset: 64
+ *   LZK_TUNE_MSM_REDUCE_RUN  buckets per lane run in the reduction tiles of
+ *                            a plain-base MSM (cfg reduce_run = 0), 1..16;
+ *                            unset: 4
  *   LZK_TUNE_NTT_BLOCK       elements per block of an NTT pass (the stages
  *                            a pass runs in shared memory), 256..4096, power
  *                            of two; unset: 2048
  *   LZK_TUNE_MSM_TABLE_WINDOW window width of MSMs over shifted-copy tables
  *                            that leave it open (batch plans with
  *                            LZK_BATCH_FIXED_BASES); unset: the cost model
+ *   LZK_TUNE_MSM_TABLE_CHUNK, LZK_TUNE_MSM_TABLE_RUN
+ *                            chunk and run of MSMs over shifted-copy tables
+ *                            (LZK_MSM_PRECOMPUTED, Groth16 provers, fixed-
+ *                            base batch plans), whose single bucket set
+ *                            wants other values than a plain MSM's per-
+ *                            window sets; unset: 64 and 4
  * The reference fixes all of these at compile time (c = 12 with 4096
  * buckets, msm.cuh:216-227; one launch per NTT stage, poly.cuh:42-63).
  * value 0 clears an entry.  A Groth16 prover and a batch plan read the table
@@ -465,6 +473,8 @@ int lzk_batch_plan_destroy(lzk_batch_plan* plan);
 #define LZK_TUNE_MSM_REDUCE_RUN 2
 #define LZK_TUNE_NTT_BLOCK      3
 #define LZK_TUNE_MSM_TABLE_WINDOW 4
+#define LZK_TUNE_MSM_TABLE_CHUNK  5
+#define LZK_TUNE_MSM_TABLE_RUN    6
 int lzk_tune_set(int knob, int group, uint32_t log_n, uint32_t value);
 /* The value in effect (the entry, or the default; 0 for an unset window). */
 uint32_t lzk_tune_get(int knob, int group, uint32_t log_n);

@@ -9,8 +9,8 @@ seeded random inputs, median of a few runs) and installs the fastest:
   run     buckets per lane run in the bucket-reduction tiles (4, 8, 16)
   ntt     elements per block of an NTT pass, i.e. how a transform's stages
           split into passes (1024, 2048, 4096)
-  table_window  window width of MSMs over shifted-copy tables (batch plans
-          with fixed bases)
+  table_*  window width, chunk and run of MSMs over shifted-copy tables
+          (provers, batch plans with fixed bases), tuned for throughput
 
 Every autotuned MSM, batch plan and prover made afterwards uses the table
 (a prover or plan reads it when it is created).  `save` / `load` keep a
@@ -27,8 +27,9 @@ from . import _capi, msm, ntt, synth
 # measured tables shipped with the package, by GPU name
 DEFAULT_TABLES = {"B200": os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning", "b200.json")}
 
-WINDOW, CHUNK, RUN, NTT_BLOCK, TABLE_WINDOW = 0, 1, 2, 3, 4
-KNOBS = {"window": WINDOW, "chunk": CHUNK, "run": RUN, "ntt": NTT_BLOCK, "table_window": TABLE_WINDOW}
+WINDOW, CHUNK, RUN, NTT_BLOCK, TABLE_WINDOW, TABLE_CHUNK, TABLE_RUN = range(7)
+KNOBS = {"window": WINDOW, "chunk": CHUNK, "run": RUN, "ntt": NTT_BLOCK, "table_window": TABLE_WINDOW,
+         "table_chunk": TABLE_CHUNK, "table_run": TABLE_RUN}
 
 
 def _time(fn, reps):
@@ -106,25 +107,54 @@ def tune_msm(group=1, log_ns=range(10, 21), spread=2, reps=3, seed=11, chunks=(3
     return out
 
 
-def tune_msm_table(group=1, log_ns=range(10, 21), widths=range(11, 19), reps=3, seed=11):
-    """window width of MSMs over shifted-copy tables (batch plans with fixed
-    bases) per size class; installs the fastest and returns
-    {log_n: (best_c, {c: ms})}"""
+def tune_msm_table(group=1, log_ns=range(10, 21), spread=3, reps=3, seed=11, total_log=20, runs=(4, 8, 16),
+                   chunks=(32, 64, 128)):
+    """window width, reduction run and chunk of MSMs over shifted-copy
+    tables, per size class, for throughput: each trial is a batch plan with
+    fixed bases holding 2^total_log points in MSMs of 2^log_n points (one
+    for the largest classes), run through its CUDA graph, so the costs of
+    many sets of buckets add up as they do in a batch.  Installs the best
+    and returns {log_n: {"window", "run", "chunk", "ms": {"c,run": ms},
+    "chunk_ms": {chunk: ms}}}"""
+    from . import batch, device
     out = {}
-    top = max(log_ns)
-    sc_all = synth.random_fr(1 << top, seed, 90)
-    bases_all = synth.fixed_base(group, synth.random_fr(1 << top, seed, 91))
+    top = max(max(log_ns), total_log)
+    sc_all = synth.random_fr(1 << top, seed, 94)
+    bases_all = synth.fixed_base(group, synth.random_fr(1 << top, seed, 95))
+    shape = (3, 4) if group == 1 else (3, 2, 4)
+    stream = torch.cuda.Stream()
     for lg in log_ns:
         n = 1 << lg
+        k = max(1, (1 << total_log) >> lg)
+        outs = [device.empty(shape) for _ in range(k)]
+
+        def trial(c):
+            plan = batch.BatchPlan(group, [(sc_all[i * n:(i + 1) * n], bases_all[i * n:(i + 1) * n], outs[i], c)
+                                           for i in range(k)], [], fixed_bases=True)
+            plan.run(use_graph=True, stream=stream)
+            ms = _time(lambda: plan.run(use_graph=True, stream=stream), reps)
+            plan.close()
+            return ms
+
+        for knob in ("table_window", "table_run", "table_chunk"):
+            set_value(knob, group, lg, 0)
+        c0 = msm.autotune_window(group, n, precomputed=True)
         res = {}
-        for c in widths:
-            w = msm.windows_for(c)
-            t = msm.precompute(group, bases_all[:n], c, w, n)
-            res[c] = _time(lambda: msm.msm_precomputed(group, sc_all[:n], t, c, w, n), reps)
-            del t
-        best = min(res, key=res.get)
-        set_value("table_window", group, lg, best)
-        out[lg] = (best, res)
+        for c in range(max(4, c0 - spread), min(20, c0 + spread) + 1):
+            for r in runs:
+                set_value("table_run", group, lg, r)
+                res[(c, r)] = trial(c)
+        c_best, r_best = min(res, key=res.get)
+        set_value("table_window", group, lg, c_best)
+        set_value("table_run", group, lg, r_best)
+        cres = {}
+        for v in chunks:
+            set_value("table_chunk", group, lg, v)
+            cres[v] = trial(c_best)
+        ch_best = min(cres, key=cres.get)
+        set_value("table_chunk", group, lg, ch_best)
+        out[lg] = {"window": c_best, "run": r_best, "chunk": ch_best,
+                   "ms": {f"{c},{r}": v for (c, r), v in res.items()}, "chunk_ms": cres}
     return out
 
 
@@ -160,8 +190,8 @@ def tune_prover(circuit, pk, mode=0, window_bits=17, chunks=(32, 64), runs=(4, 8
     def install(chunk, run):
         for g, lgs in classes.items():
             for lg in lgs:
-                set_value("chunk", g, lg, chunk)
-                set_value("run", g, lg, run)
+                set_value("table_chunk", g, lg, chunk)
+                set_value("table_run", g, lg, run)
 
     res = {}
     for chunk in chunks:
@@ -191,7 +221,7 @@ def current(groups=(1, 2), log_ns=range(0, 33)):
     t = {"msm": {}, "ntt": {}}
     for g in groups:
         t["msm"][str(g)] = {k: {str(lg): get_value(k, g, lg) for lg in log_ns}
-                            for k in ("window", "chunk", "run", "table_window")}
+                            for k in ("window", "chunk", "run", "table_window", "table_chunk", "table_run")}
     t["ntt"] = {str(lg): get_value("ntt", 0, lg) for lg in log_ns}
     return t
 

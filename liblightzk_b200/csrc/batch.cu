@@ -275,8 +275,8 @@ static int create_plan(const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_des
     // the plan's largest MSM picks the accumulation chunk and reduction run
     size_t largest = 0;
     for (size_t i = 0; i < n_msm; i++) largest = std::max(largest, msms[i].n);
-    p->chunk = tune_chunk(p->group, largest);
-    p->run = tune_run(p->group, largest);
+    p->chunk = tune_chunk(p->group, largest, p->fixed);
+    p->run = tune_run(p->group, largest, p->fixed);
     p->chunks = (p->max_entries + p->chunk - 1) / p->chunk;
     for (auto& g : p->wgroups) {
         uint64_t nb = 1ull << (g.c - 1);

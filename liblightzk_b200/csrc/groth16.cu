@@ -287,8 +287,8 @@ static int create(const lzk_groth16_circuit* c, const lzk_groth16_pk* pk, int mo
     for (int i = 0; i < 3; i++) {
         size_t n = i == 0 ? p->tn[2] : p->n_vars;
         int group = i == 2 ? 2 : 1;
-        p->chunk[i] = tune_chunk(group, n);
-        p->run[i] = tune_run(group, n);
+        p->chunk[i] = tune_chunk(group, n, true);
+        p->run[i] = tune_run(group, n, true);
     }
 
     LZK_TRY(ctx_create(p, false, &p->ctx0));

@@ -33,14 +33,16 @@ struct MsmPlan {
 inline uint32_t windows_for(uint32_t c) { return (255 + c - 1) / c; }
 
 // accumulation chunk and reduction run of an MSM of n points in group g:
-// cfg's values, else the tuning table's
+// cfg's values, else the tuning table's (plain bases, or tables with
+// LZK_MSM_PRECOMPUTED)
+inline bool msm_shared(const lzk_msm_cfg* cfg) { return cfg && (cfg->flags & LZK_MSM_PRECOMPUTED); }
 inline uint32_t msm_chunk(const lzk_msm_cfg* cfg, int group, size_t n)
 {
-    return cfg && cfg->acc_chunk ? cfg->acc_chunk : tune_chunk(group, n);
+    return cfg && cfg->acc_chunk ? cfg->acc_chunk : tune_chunk(group, n, msm_shared(cfg));
 }
 inline uint32_t msm_run(const lzk_msm_cfg* cfg, int group, size_t n)
 {
-    return cfg && cfg->reduce_run ? cfg->reduce_run : tune_run(group, n);
+    return cfg && cfg->reduce_run ? cfg->reduce_run : tune_run(group, n, msm_shared(cfg));
 }
 
 template <class Gp>

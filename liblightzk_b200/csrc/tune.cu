@@ -8,7 +8,9 @@
 // the table from timings on the device.  An unset entry (0) means the
 // built-in default: the cost model's window width, 64 entries per
 // accumulation thread, runs of 4 buckets per lane, 2048 elements per NTT
-// block.
+// block.  MSMs over shifted-copy tables (one bucket set for all windows)
+// have their own window, chunk and run entries: their best values differ
+// from those of plain-base MSMs of the same size.
 #include "common.cuh"
 #include "tune.cuh"
 #include <atomic>
@@ -30,15 +32,15 @@ uint32_t tune_lookup(int knob, int group, size_t n)
     return g_tune[knob][group][log2_ceil(n)].load(std::memory_order_relaxed);
 }
 
-uint32_t tune_chunk(int group, size_t n)
+uint32_t tune_chunk(int group, size_t n, bool shared)
 {
-    uint32_t v = tune_lookup(LZK_TUNE_MSM_CHUNK, group, n);
+    uint32_t v = tune_lookup(shared ? LZK_TUNE_MSM_TABLE_CHUNK : LZK_TUNE_MSM_CHUNK, group, n);
     return v ? v : kDefaultChunk;
 }
 
-uint32_t tune_run(int group, size_t n)
+uint32_t tune_run(int group, size_t n, bool shared)
 {
-    uint32_t v = tune_lookup(LZK_TUNE_MSM_REDUCE_RUN, group, n);
+    uint32_t v = tune_lookup(shared ? LZK_TUNE_MSM_TABLE_RUN : LZK_TUNE_MSM_REDUCE_RUN, group, n);
     return v ? v : kDefaultRun;
 }
 
@@ -56,8 +58,10 @@ bool tune_valid(int knob, uint32_t v)
     switch (knob) {
         case LZK_TUNE_MSM_WINDOW:
         case LZK_TUNE_MSM_TABLE_WINDOW: return v >= 2 && v <= 24;
-        case LZK_TUNE_MSM_CHUNK: return pow2(v) && v >= kMinChunk && v <= kMaxChunk;
-        case LZK_TUNE_MSM_REDUCE_RUN: return pow2(v) && v <= kMaxRun;
+        case LZK_TUNE_MSM_CHUNK:
+        case LZK_TUNE_MSM_TABLE_CHUNK: return pow2(v) && v >= kMinChunk && v <= kMaxChunk;
+        case LZK_TUNE_MSM_REDUCE_RUN:
+        case LZK_TUNE_MSM_TABLE_RUN: return pow2(v) && v <= kMaxRun;
         case LZK_TUNE_NTT_BLOCK: return pow2(v) && v >= kMinNttBlock && v <= kMaxNttBlock;
         default: return false;
     }
@@ -85,8 +89,10 @@ uint32_t lzk_tune_get(int knob, int group, uint32_t log_n)
     if (group < 1 || group > 2) return 0;
     size_t n = size_t(1) << (log_n < 63 ? log_n : 62);
     switch (knob) {
-        case LZK_TUNE_MSM_CHUNK: return tune_chunk(group, n);
-        case LZK_TUNE_MSM_REDUCE_RUN: return tune_run(group, n);
+        case LZK_TUNE_MSM_CHUNK: return tune_chunk(group, n, false);
+        case LZK_TUNE_MSM_REDUCE_RUN: return tune_run(group, n, false);
+        case LZK_TUNE_MSM_TABLE_CHUNK: return tune_chunk(group, n, true);
+        case LZK_TUNE_MSM_TABLE_RUN: return tune_run(group, n, true);
         default: return g_tune[knob][group][log_n].load(std::memory_order_relaxed);
     }
 }

@@ -9,7 +9,7 @@ import pytest
 from helpers import bases, same_point, scalars
 from oracle import FR
 
-WINDOW, CHUNK, RUN, NTT_BLOCK = 0, 1, 2, 3
+WINDOW, CHUNK, RUN, NTT_BLOCK, TABLE_WINDOW, TABLE_CHUNK, TABLE_RUN = range(7)
 
 
 def _lib():
@@ -33,6 +33,14 @@ def test_defaults_validation_and_clearing():
     assert L.lzk_tune_set(NTT_BLOCK, 0, 12, 0) == 0 and L.lzk_tune_get(NTT_BLOCK, 0, 12) == 2048
     assert L.lzk_msm_set_window(1, 14, 9) == 0 and L.lzk_tune_get(WINDOW, 1, 14) == 9
     assert L.lzk_msm_set_window(1, 14, 0) == 0
+    # tables have their own entries
+    assert L.lzk_tune_get(TABLE_CHUNK, 1, 20) == 64 and L.lzk_tune_get(TABLE_RUN, 1, 20) == 4
+    assert L.lzk_tune_set(TABLE_RUN, 1, 20, 8) == 0 and L.lzk_tune_get(TABLE_RUN, 1, 20) == 8
+    assert L.lzk_tune_get(RUN, 1, 20) == 4
+    assert L.lzk_tune_set(TABLE_RUN, 1, 20, 0) == 0
+    assert L.lzk_tune_set(TABLE_WINDOW, 2, 18, 17) == 0 and L.lzk_tune_get(TABLE_WINDOW, 2, 18) == 17
+    assert L.lzk_tune_set(TABLE_WINDOW, 2, 18, 0) == 0
+    assert L.lzk_tune_set(TABLE_CHUNK, 1, 20, 24) == -1 and L.lzk_tune_set(7, 1, 20, 4) == -1
 
 
 @pytest.mark.gpu
@@ -52,16 +60,16 @@ def test_msm_knobs_keep_results(cuda, orc, rng_state, group):
                 for c in (7, 12):
                     got = device.to_host(msm.msm(group, ds, db, window_bits=c))
                     assert same_point(orc, group, got, want), (chunk, run, c)
-        # a precomputed table too (one shared bucket set)
+        # a precomputed table too (one shared bucket set, its own entries)
         t = msm.precompute(group, db, 13, msm.windows_for(13), n)
         for chunk, run in ((16, 16), (256, 1)):
-            L.lzk_tune_set(CHUNK, group, lg, chunk)
-            L.lzk_tune_set(RUN, group, lg, run)
+            L.lzk_tune_set(TABLE_CHUNK, group, lg, chunk)
+            L.lzk_tune_set(TABLE_RUN, group, lg, run)
             got = device.to_host(msm.msm_precomputed(group, ds, t, 13, msm.windows_for(13), n))
             assert same_point(orc, group, got, want), (chunk, run, "table")
     finally:
-        L.lzk_tune_set(CHUNK, group, lg, 0)
-        L.lzk_tune_set(RUN, group, lg, 0)
+        for k in (CHUNK, RUN, TABLE_CHUNK, TABLE_RUN):
+            L.lzk_tune_set(k, group, lg, 0)
 
 
 @pytest.mark.gpu
