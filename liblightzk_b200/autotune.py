@@ -10,7 +10,7 @@ seeded random inputs, median of a few runs) and installs the fastest:
   ntt     elements per block of an NTT pass, i.e. how a transform's stages
           split into passes (1024, 2048, 4096)
   table_*  window width, chunk and run of MSMs over shifted-copy tables
-          (provers, batch plans with fixed bases), tuned for throughput
+          (provers, batch plans with fixed bases)
 
 Every autotuned MSM, batch plan and prover made afterwards uses the table
 (a prover or plan reads it when it is created).  `save` / `load` keep a
@@ -107,52 +107,40 @@ def tune_msm(group=1, log_ns=range(10, 21), spread=2, reps=3, seed=11, chunks=(3
     return out
 
 
-def tune_msm_table(group=1, log_ns=range(10, 21), spread=3, reps=3, seed=11, total_log=20, runs=(4, 8, 16),
-                   chunks=(32, 64, 128)):
-    """window width, reduction run and chunk of MSMs over shifted-copy
-    tables, per size class, for throughput: each trial is a batch plan with
-    fixed bases holding 2^total_log points in MSMs of 2^log_n points (one
-    for the largest classes), run through its CUDA graph, so the costs of
-    many sets of buckets add up as they do in a batch.  Installs the best
+def tune_msm_table(group=1, log_ns=range(10, 21), spread=2, reps=3, seed=11, runs=(4, 8, 16), chunks=(32, 64, 128)):
+    """window width and reduction run (together), then chunk, of an MSM over
+    a shifted-copy table, per size class, timing one MSM of 2^log_n points
+    (the table of each width built outside the timing); installs the best
     and returns {log_n: {"window", "run", "chunk", "ms": {"c,run": ms},
     "chunk_ms": {chunk: ms}}}"""
-    from . import batch, device
     out = {}
-    top = max(max(log_ns), total_log)
+    top = max(log_ns)
     sc_all = synth.random_fr(1 << top, seed, 94)
     bases_all = synth.fixed_base(group, synth.random_fr(1 << top, seed, 95))
-    shape = (3, 4) if group == 1 else (3, 2, 4)
-    stream = torch.cuda.Stream()
     for lg in log_ns:
         n = 1 << lg
-        k = max(1, (1 << total_log) >> lg)
-        outs = [device.empty(shape) for _ in range(k)]
-
-        def trial(c):
-            plan = batch.BatchPlan(group, [(sc_all[i * n:(i + 1) * n], bases_all[i * n:(i + 1) * n], outs[i], c)
-                                           for i in range(k)], [], fixed_bases=True)
-            plan.run(use_graph=True, stream=stream)
-            ms = _time(lambda: plan.run(use_graph=True, stream=stream), reps)
-            plan.close()
-            return ms
-
+        s, b = sc_all[:n], bases_all[:n]
         for knob in ("table_window", "table_run", "table_chunk"):
             set_value(knob, group, lg, 0)
         c0 = msm.autotune_window(group, n, precomputed=True)
-        res = {}
+        res, tabs = {}, {}
         for c in range(max(4, c0 - spread), min(20, c0 + spread) + 1):
+            w = msm.windows_for(c)
+            tabs[c] = msm.precompute(group, b, c, w, n)
             for r in runs:
                 set_value("table_run", group, lg, r)
-                res[(c, r)] = trial(c)
+                res[(c, r)] = _time(lambda c=c, w=w: msm.msm_precomputed(group, s, tabs[c], c, w, n), reps)
         c_best, r_best = min(res, key=res.get)
         set_value("table_window", group, lg, c_best)
         set_value("table_run", group, lg, r_best)
+        w = msm.windows_for(c_best)
         cres = {}
         for v in chunks:
             set_value("table_chunk", group, lg, v)
-            cres[v] = trial(c_best)
+            cres[v] = _time(lambda: msm.msm_precomputed(group, s, tabs[c_best], c_best, w, n), reps)
         ch_best = min(cres, key=cres.get)
         set_value("table_chunk", group, lg, ch_best)
+        del tabs
         out[lg] = {"window": c_best, "run": r_best, "chunk": ch_best,
                    "ms": {f"{c},{r}": v for (c, r), v in res.items()}, "chunk_ms": cres}
     return out

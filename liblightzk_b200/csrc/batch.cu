@@ -41,12 +41,13 @@ struct lzk_batch_plan {
     uint64_t table_pts = 0;
     size_t table_bytes = 0;
     std::vector<BDesc> msm;            // sorted by window width
-    struct WGroup { uint32_t c; uint64_t bucket_base, windows; };
+    struct WGroup { uint32_t c; uint64_t bucket_base, windows; size_t largest; uint32_t run; };
     std::vector<WGroup> wgroups;
     struct NGroup { uint32_t k; int dir; uint32_t count; lzk::Fr** ptrs; };
     std::vector<NGroup> ngroups;
     uint64_t total_pts = 0, total_buckets = 0, total_windows = 0, max_entries = 0, chunks = 0, lvl = 0;
-    uint32_t chunk = 0, run = 0;       // accumulation chunk, reduction run (tuning table, at creation)
+    uint32_t chunk = 0, run = 0;       // accumulation chunk, reduction run (tuning table, at creation; the
+                                       // width groups take their own runs)
     char* ws = nullptr;
     size_t ws_bytes = 0;
     BDesc* d_desc = nullptr;
@@ -184,7 +185,7 @@ static int run_plan(lzk_batch_plan* p, cudaStream_t st)
             LZK_TRY(reduce_buckets<F>(bsum + wg.bucket_base, p->off + wg.bucket_base, (uint32_t)wg.windows,
                                       1u << (wg.c - 1), static_cast<X*>(p->lr[0]), static_cast<X*>(p->la[0]),
                                       static_cast<X*>(p->lr[1]), static_cast<X*>(p->la[1]),
-                                      static_cast<X*>(p->wres) + wdone, st, p->run));
+                                      static_cast<X*>(p->wres) + wdone, st, wg.run));
             wdone += wg.windows;
         }
         trace_end(tr, st);
@@ -264,8 +265,9 @@ static int create_plan(const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_des
         p->total_buckets += (uint64_t)d.hw * d.nb;
         p->total_windows += d.hw;
         p->max_entries += m.n * (uint64_t)d.W;
-        if (p->wgroups.empty() || p->wgroups.back().c != d.c) p->wgroups.push_back({d.c, d.bucket_base, 0});
+        if (p->wgroups.empty() || p->wgroups.back().c != d.c) p->wgroups.push_back({d.c, d.bucket_base, 0, 0, 0});
         p->wgroups.back().windows += d.hw;
+        p->wgroups.back().largest = std::max<size_t>(p->wgroups.back().largest, m.n);
         ptsoff.push_back(d.pts_off);
         p->msm.push_back(d);
     }
@@ -277,6 +279,8 @@ static int create_plan(const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_des
     for (size_t i = 0; i < n_msm; i++) largest = std::max(largest, msms[i].n);
     p->chunk = tune_chunk(p->group, largest, p->fixed);
     p->run = tune_run(p->group, largest, p->fixed);
+    // each width group reduces with the run of its own largest MSM's size class
+    for (auto& g : p->wgroups) g.run = tune_run(p->group, g.largest, p->fixed);
     p->chunks = (p->max_entries + p->chunk - 1) / p->chunk;
     for (auto& g : p->wgroups) {
         uint64_t nb = 1ull << (g.c - 1);
