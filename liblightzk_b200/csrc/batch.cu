@@ -41,7 +41,7 @@ struct lzk_batch_plan {
     uint64_t table_pts = 0;
     size_t table_bytes = 0;
     std::vector<BDesc> msm;            // sorted by window width
-    struct WGroup { uint32_t c; uint64_t bucket_base, windows; size_t largest; uint32_t run; };
+    struct WGroup { uint32_t c; uint64_t bucket_base, windows; size_t largest; uint32_t run; uint64_t scratch_off; };
     std::vector<WGroup> wgroups;
     struct NGroup { uint32_t k; int dir; uint32_t count; lzk::Fr** ptrs; };
     std::vector<NGroup> ngroups;
@@ -178,16 +178,19 @@ static int run_plan(lzk_batch_plan* p, cudaStream_t st)
         k_fixup_large<F><<<sm_count() * 2, fx_threads, fx_threads * sizeof(X), st>>>(p->off, p->chunk, bsum, static_cast<X*>(p->head),
                                                                              static_cast<X*>(p->tail), p->large); note_launch();
         trace_end(tr, st);
-        // one bucket reduction per window width
+        // the bucket reductions of all window widths, in the same four launches
         tr = trace_begin("batch_msm_reduce", st);
+        std::vector<RedJob<F>> jobs;
         uint64_t wdone = 0;
         for (auto& wg : p->wgroups) {
-            LZK_TRY(reduce_buckets<F>(bsum + wg.bucket_base, p->off + wg.bucket_base, (uint32_t)wg.windows,
-                                      1u << (wg.c - 1), static_cast<X*>(p->lr[0]), static_cast<X*>(p->la[0]),
-                                      static_cast<X*>(p->lr[1]), static_cast<X*>(p->la[1]),
-                                      static_cast<X*>(p->wres) + wdone, st, wg.run));
+            const uint64_t o = wg.scratch_off;
+            jobs.push_back(red_job<F>(bsum + wg.bucket_base, p->off + wg.bucket_base, (uint32_t)wg.windows,
+                                      1u << (wg.c - 1), wg.run, static_cast<X*>(p->lr[0]) + o,
+                                      static_cast<X*>(p->la[0]) + o, static_cast<X*>(p->lr[1]) + o,
+                                      static_cast<X*>(p->la[1]) + o, static_cast<X*>(p->wres) + wdone));
             wdone += wg.windows;
         }
+        LZK_TRY(reduce_jobs<F>(jobs.data(), jobs.size(), st));
         trace_end(tr, st);
     }
     if (count) {
@@ -265,7 +268,7 @@ static int create_plan(const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_des
         p->total_buckets += (uint64_t)d.hw * d.nb;
         p->total_windows += d.hw;
         p->max_entries += m.n * (uint64_t)d.W;
-        if (p->wgroups.empty() || p->wgroups.back().c != d.c) p->wgroups.push_back({d.c, d.bucket_base, 0, 0, 0});
+        if (p->wgroups.empty() || p->wgroups.back().c != d.c) p->wgroups.push_back({d.c, d.bucket_base, 0, 0, 0, 0});
         p->wgroups.back().windows += d.hw;
         p->wgroups.back().largest = std::max<size_t>(p->wgroups.back().largest, m.n);
         ptsoff.push_back(d.pts_off);
@@ -282,9 +285,11 @@ static int create_plan(const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_des
     // each width group reduces with the run of its own largest MSM's size class
     for (auto& g : p->wgroups) g.run = tune_run(p->group, g.largest, p->fixed);
     p->chunks = (p->max_entries + p->chunk - 1) / p->chunk;
+    // every width group reduces in the same launches, each in its own slice
+    // of the reduction scratch
     for (auto& g : p->wgroups) {
-        uint64_t nb = 1ull << (g.c - 1);
-        p->lvl = std::max<uint64_t>(p->lvl, g.windows * (nb > kLevelL ? nb / kLevelL : 1));
+        g.scratch_off = p->lvl;
+        p->lvl += red_scratch_points((uint32_t)g.windows, 1u << (g.c - 1));
     }
     uint64_t B = std::max<uint64_t>(p->total_buckets, 1);
     Carver cv;

@@ -298,7 +298,8 @@ __device__ __forceinline__ XYZZ<F> shfl_pt(const XYZZ<F>& x, uint32_t lane)
 //   W = sum_u t_u + L sum_u u R_u = T + sum_{i < log P} 2^(i + log L) G_i,
 // where R_u is the sum of tile u, t_u = sum_j (j+1) B_{uL+j} its locally
 // weighted sum, T = sum_u t_u and G_i = sum of the R_u with bit i of u set
-// (bit slices of the tile index).  Four launches:
+// (bit slices of the tile index).  Four launches, each over the items of
+// any number of jobs (reduce_jobs):
 //   k_red_tile     one warp per tile (below);
 //   k_red_slices   one warp per 32 members of one of the 1 + log P sums T,
 //                  G_0, G_1, ... (xor-shuffle tree);
@@ -319,40 +320,6 @@ __device__ __forceinline__ XYZZ<F> shfl_pt(const XYZZ<F>& x, uint32_t lane)
 //   R_u = S_0,   t_u = sum_j (t_j + r [j >= 1] S_j).
 // About 4.75 additions per bucket for r = 4, against 10 for a warp scan over
 // single buckets (r = 1).
-template <class F>
-__global__ void __launch_bounds__(128) k_red_tile(const XYZZ<F>* __restrict__ bsum, const uint32_t* __restrict__ off,
-                                                  uint32_t wb, uint32_t m, uint32_t L, uint32_t r,
-                                                  XYZZ<F>* __restrict__ R, XYZZ<F>* __restrict__ T)
-{
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t nl = L / r;   // active lanes
-    const uint64_t total = (uint64_t)wb * (m / L);
-    for (uint64_t tile = gtid() >> 5; tile < total; tile += gstride() >> 5) {
-        XYZZ<F> s = xyzz_inf<F>(), t = xyzz_inf<F>();
-        if (lane < nl) {
-            const size_t k0 = (size_t)tile * L + (size_t)lane * r;   // = w m + u L + j r
-            for (int i = (int)r - 1; i >= 0; i--) {
-                size_t k = k0 + (uint32_t)i;
-                if (off[k] != off[k + 1]) s = xyzz_add_cold(s, ld_elem(bsum + k));
-                t = xyzz_add_cold(t, s);
-            }
-        }
-        XYZZ<F> S = s;
-        for (uint32_t d = 1; d < nl; d <<= 1) {
-            XYZZ<F> o = shfl_down_pt(S, d);
-            if (lane + d < nl) S = xyzz_add_cold(S, o);
-        }
-        XYZZ<F> U = (lane >= 1 && lane < nl) ? S : xyzz_inf<F>();
-        for (uint32_t q = r; q > 1; q >>= 1) U = xyzz_dbl_cold(U);
-        XYZZ<F> V = xyzz_add_cold(t, U);
-        for (uint32_t d = nl >> 1; d > 0; d >>= 1) V = xyzz_add_cold(V, shfl_xor_pt(V, d));
-        if (lane == 0) {
-            st_elem(R + tile, S);
-            st_elem(T + tile, V);
-        }
-    }
-}
-
 struct RedShape {
     uint32_t r, L, lgL, P, lg;   // buckets per lane run, tile size, log2 L, tiles per set, log2 P
     uint32_t cT, cG, NP, NS;     // chunks of T, chunks of each G_i, partials and sums per set
@@ -381,38 +348,106 @@ __device__ __forceinline__ uint32_t slice_member(uint32_t v, uint32_t i)
     return ((v >> i) << (i + 1)) | (1u << i) | (v & ((1u << i) - 1));
 }
 
+// One reduction job: wb sets of m buckets (bsum / off indexed w m + k) into
+// win[0..wb), with scratch R, T, part, scaled of its own (at least wb * P
+// points each; NP, NS <= P), so that the jobs of several window widths (a
+// batch plan's width groups) run in the same launches.  s_* is the job's
+// first item in each launch's item space (the items of all jobs laid end to
+// end: tiles wb P, slice partials wb NP, sums wb NS, sets wb).
 template <class F>
-__global__ void __launch_bounds__(128) k_red_slices(const XYZZ<F>* __restrict__ R, const XYZZ<F>* __restrict__ T,
-                                                    uint32_t wb, RedShape sh, XYZZ<F>* __restrict__ part)
+struct RedJob {
+    const XYZZ<F>* bsum;
+    const uint32_t* off;
+    XYZZ<F> *R, *T, *part, *scaled, *win;
+    uint32_t wb, m;
+    RedShape sh;
+    uint64_t s_tile, s_np, s_ns, s_w;
+};
+constexpr uint32_t kMaxRedJobs = 20;   // a kernel parameter of about 3 KB
+template <class F>
+struct RedJobs {
+    uint32_t count;
+    RedJob<F> g[kMaxRedJobs];
+};
+
+// the job whose items include `item` (jobs in item order)
+template <class F>
+__device__ __forceinline__ uint32_t red_job_of(const RedJobs<F>& jobs, uint64_t item, uint64_t RedJob<F>::*start)
+{
+    uint32_t j = 0;
+    while (j + 1 < jobs.count && item >= jobs.g[j + 1].*start) j++;
+    return j;
+}
+
+template <class F>
+__global__ void __launch_bounds__(128) k_red_tile(const __grid_constant__ RedJobs<F> jobs, uint64_t total)
 {
     const uint32_t lane = threadIdx.x & 31;
-    const uint64_t total = (uint64_t)wb * sh.NP;
-    for (uint64_t g = gtid() >> 5; g < total; g += gstride() >> 5) {
+    for (uint64_t item = gtid() >> 5; item < total; item += gstride() >> 5) {
+        const RedJob<F>& J = jobs.g[red_job_of(jobs, item, &RedJob<F>::s_tile)];
+        const uint64_t tile = item - J.s_tile;
+        const uint32_t L = J.sh.L, r = J.sh.r;
+        const uint32_t nl = L / r;   // active lanes
+        XYZZ<F> s = xyzz_inf<F>(), t = xyzz_inf<F>();
+        if (lane < nl) {
+            const size_t k0 = (size_t)tile * L + (size_t)lane * r;   // = w m + u L + j r
+            for (int i = (int)r - 1; i >= 0; i--) {
+                size_t k = k0 + (uint32_t)i;
+                if (J.off[k] != J.off[k + 1]) s = xyzz_add_cold(s, ld_elem(J.bsum + k));
+                t = xyzz_add_cold(t, s);
+            }
+        }
+        XYZZ<F> S = s;
+        for (uint32_t d = 1; d < nl; d <<= 1) {
+            XYZZ<F> o = shfl_down_pt(S, d);
+            if (lane + d < nl) S = xyzz_add_cold(S, o);
+        }
+        XYZZ<F> U = (lane >= 1 && lane < nl) ? S : xyzz_inf<F>();
+        for (uint32_t q = r; q > 1; q >>= 1) U = xyzz_dbl_cold(U);
+        XYZZ<F> V = xyzz_add_cold(t, U);
+        for (uint32_t d = nl >> 1; d > 0; d >>= 1) V = xyzz_add_cold(V, shfl_xor_pt(V, d));
+        if (lane == 0) {
+            st_elem(J.R + tile, S);
+            st_elem(J.T + tile, V);
+        }
+    }
+}
+
+
+template <class F>
+__global__ void __launch_bounds__(128) k_red_slices(const __grid_constant__ RedJobs<F> jobs, uint64_t total)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint64_t item = gtid() >> 5; item < total; item += gstride() >> 5) {
+        const RedJob<F>& J = jobs.g[red_job_of(jobs, item, &RedJob<F>::s_np)];
+        const RedShape& sh = J.sh;
+        const uint64_t g = item - J.s_np;
         uint32_t w = (uint32_t)(g / sh.NP), q = (uint32_t)(g % sh.NP);
         const size_t base = (size_t)w * sh.P;
         XYZZ<F> x = xyzz_inf<F>();
         if (q < sh.cT) {
             uint32_t v = q * 32 + lane;
-            if (v < sh.P) x = ld_elem(T + base + v);
+            if (v < sh.P) x = ld_elem(J.T + base + v);
         } else {
             uint32_t i = (q - sh.cT) / sh.cG, v = ((q - sh.cT) % sh.cG) * 32 + lane;
-            if (v < sh.P / 2) x = ld_elem(R + base + slice_member(v, i));
+            if (v < sh.P / 2) x = ld_elem(J.R + base + slice_member(v, i));
         }
         for (uint32_t d = 16; d > 0; d >>= 1) x = xyzz_add_cold(x, shfl_xor_pt(x, d));
-        if (lane == 0) st_elem(part + g, x);
+        if (lane == 0) st_elem(J.part + g, x);
     }
 }
 
 template <class F>
-__global__ void __launch_bounds__(128) k_red_scale(const XYZZ<F>* __restrict__ part, uint32_t wb, RedShape sh,
-                                                   XYZZ<F>* __restrict__ scaled)
+__global__ void __launch_bounds__(128) k_red_scale(const __grid_constant__ RedJobs<F> jobs, uint64_t total)
 {
     const uint32_t lane = threadIdx.x & 31;
-    const uint64_t total = (uint64_t)wb * sh.NS;
-    for (uint64_t g = gtid() >> 5; g < total; g += gstride() >> 5) {
+    for (uint64_t item = gtid() >> 5; item < total; item += gstride() >> 5) {
+        const RedJob<F>& J = jobs.g[red_job_of(jobs, item, &RedJob<F>::s_ns)];
+        const RedShape& sh = J.sh;
+        const uint64_t g = item - J.s_ns;
         uint32_t w = (uint32_t)(g / sh.NS), s = (uint32_t)(g % sh.NS);
         uint32_t first = s == 0 ? 0 : sh.cT + (s - 1) * sh.cG, cnt = s == 0 ? sh.cT : sh.cG;
-        const XYZZ<F>* src = part + (size_t)w * sh.NP + first;
+        const XYZZ<F>* src = J.part + (size_t)w * sh.NP + first;
         XYZZ<F> x = xyzz_inf<F>();
         for (uint32_t c = lane; c < cnt; c += 32) x = xyzz_add_cold(x, ld_elem(src + c));
         for (uint32_t d = 16; d > 0; d >>= 1) x = xyzz_add_cold(x, shfl_xor_pt(x, d));
@@ -422,35 +457,75 @@ __global__ void __launch_bounds__(128) k_red_scale(const XYZZ<F>* __restrict__ p
         x = shfl_pt(x, 0);
         uint32_t dbls = s == 0 ? 0 : s - 1 + sh.lgL;
         for (uint32_t d = 0; d < dbls; d++) x = xyzz_dbl_warp(x);
-        if (lane == 0) st_elem(scaled + g, x);
+        if (lane == 0) st_elem(J.scaled + g, x);
     }
 }
 
 template <class F>
-__global__ void __launch_bounds__(128) k_red_combine(const XYZZ<F>* __restrict__ scaled, uint32_t wb, uint32_t NS,
-                                                     XYZZ<F>* __restrict__ win)
+__global__ void __launch_bounds__(128) k_red_combine(const __grid_constant__ RedJobs<F> jobs, uint64_t total)
 {
     const uint32_t lane = threadIdx.x & 31;
-    for (uint64_t w = gtid() >> 5; w < wb; w += gstride() >> 5) {
-        XYZZ<F> x = lane < NS ? ld_elem(scaled + w * NS + lane) : xyzz_inf<F>();
+    for (uint64_t item = gtid() >> 5; item < total; item += gstride() >> 5) {
+        const RedJob<F>& J = jobs.g[red_job_of(jobs, item, &RedJob<F>::s_w)];
+        const uint64_t w = item - J.s_w;
+        const uint32_t NS = J.sh.NS;
+        XYZZ<F> x = lane < NS ? ld_elem(J.scaled + w * NS + lane) : xyzz_inf<F>();
         for (uint32_t d = 16; d > 0; d >>= 1) x = xyzz_add_cold(x, shfl_xor_pt(x, d));
-        if (lane == 0) st_elem(win + w, x);
+        if (lane == 0) st_elem(J.win + w, x);
     }
 }
 
+// Scratch points each of R, T, part and scaled needs for wb sets of m
+// buckets (any run: P <= max(1, m / kLevelL), NP, NS <= P).
+inline size_t red_scratch_points(uint32_t wb, uint32_t m) { return (size_t)wb * (m > kLevelL ? m / kLevelL : 1); }
+
+template <class F>
+RedJob<F> red_job(const XYZZ<F>* bsum, const uint32_t* off, uint32_t wb, uint32_t m, uint32_t run, XYZZ<F>* R,
+                  XYZZ<F>* T, XYZZ<F>* part, XYZZ<F>* scaled, XYZZ<F>* win)
+{
+    RedJob<F> j{};
+    j.bsum = bsum; j.off = off; j.R = R; j.T = T; j.part = part; j.scaled = scaled; j.win = win;
+    j.wb = wb; j.m = m;
+    j.sh = red_shape(m, run);
+    return j;
+}
+
+// The weighted sums of every job, four launches for all of them (in rounds
+// of kMaxRedJobs jobs).  A job's win may alias its R.
+template <class F>
+int reduce_jobs(RedJob<F>* jv, size_t n, cudaStream_t st)
+{
+    for (size_t b = 0; b < n; b += kMaxRedJobs) {
+        RedJobs<F> jobs{};
+        jobs.count = (uint32_t)(n - b < kMaxRedJobs ? n - b : kMaxRedJobs);
+        uint64_t tiles = 0, nps = 0, nss = 0, sets = 0;
+        for (uint32_t i = 0; i < jobs.count; i++) {
+            RedJob<F> j = jv[b + i];
+            j.s_tile = tiles; j.s_np = nps; j.s_ns = nss; j.s_w = sets;
+            tiles += (uint64_t)j.wb * j.sh.P;
+            nps += (uint64_t)j.wb * j.sh.NP;
+            nss += (uint64_t)j.wb * j.sh.NS;
+            sets += j.wb;
+            jobs.g[i] = j;
+        }
+        k_red_tile<F><<<grid_for(tiles * 32, 128), 128, 0, st>>>(jobs, tiles); note_launch();
+        k_red_slices<F><<<grid_for(nps * 32, 128), 128, 0, st>>>(jobs, nps); note_launch();
+        k_red_scale<F><<<grid_for(nss * 32, 128), 128, 0, st>>>(jobs, nss); note_launch();
+        k_red_combine<F><<<grid_for(sets * 32, 128), 128, 0, st>>>(jobs, sets); note_launch();
+        LZK_TRY(launch_status());
+    }
+    return LZK_OK;
+}
+
 // W_w of wb sets of m buckets (bsum / off indexed w m + k) into win[0..wb).
-// Scratch: R, T of at least wb * P points each (P <= max(1, m / 32)); part
-// and scaled fit in the same size (NP, NS <= P).  win may alias R.
+// Scratch: R, T, part, scaled of red_scratch_points(wb, m) points each.  win
+// may alias R.
 template <class F>
 int reduce_buckets(const XYZZ<F>* bsum, const uint32_t* off, uint32_t wb, uint32_t m, XYZZ<F>* R, XYZZ<F>* T,
                    XYZZ<F>* part, XYZZ<F>* scaled, XYZZ<F>* win, cudaStream_t st, uint32_t run = kDefaultRun)
 {
-    RedShape sh = red_shape(m, run);
-    k_red_tile<F><<<grid_for((size_t)wb * sh.P * 32, 128), 128, 0, st>>>(bsum, off, wb, m, sh.L, sh.r, R, T); note_launch();
-    k_red_slices<F><<<grid_for((size_t)wb * sh.NP * 32, 128), 128, 0, st>>>(R, T, wb, sh, part); note_launch();
-    k_red_scale<F><<<grid_for((size_t)wb * sh.NS * 32, 128), 128, 0, st>>>(part, wb, sh, scaled); note_launch();
-    k_red_combine<F><<<grid_for((size_t)wb * 32, 128), 128, 0, st>>>(scaled, wb, sh.NS, win); note_launch();
-    return launch_status();
+    RedJob<F> j = red_job<F>(bsum, off, wb, m, run, R, T, part, scaled, win);
+    return reduce_jobs<F>(&j, 1, st);
 }
 
 // Horner over the bucket sets' weighted sums (plain bases), or the
