@@ -490,7 +490,8 @@ def run_tune_case(args):
     print(json.dumps({"case": "tune", "seconds": time.time() - t0,
                       "msm_g1": {lg: {k: v[k] for k in ("window", "run", "chunk")} for lg, v in t1.items()},
                       "msm_g2": {lg: {k: v[k] for k in ("window", "run", "chunk")} for lg, v in t2.items()},
-                      "msm_g1_table": {lg: {k: v[k] for k in ("window", "run", "chunk")} for lg, v in tt.items()},
+                      "msm_g1_table": {lg: {k: v[k] for k in ("window", "run", "chunk", "ms", "chunk_ms")}
+                                       for lg, v in tt.items()},
                       "ntt_block": {lg: {"best": v[0], "ms": v[1]} for lg, v in tn.items()},
                       "prover_ms_per_proof": {f"chunk {c}, run {r}": ms for (c, r), ms in tp.items()}}), flush=True)
 
@@ -701,14 +702,16 @@ def main():
         ms_total, e2e_ms = float(t[0]), float(t[1])
 
     # ---------------- G1 MSM at 2^20 (precomputed table, as msm-check.cu) ----------------
-    g1_ms = g1_plain_ms = None
+    g1_ms = g1_plain_ms = g1_window = None
     iso_ms = iso_n = iso_pts = 0
     other = {}
     if rank == 0:
         n = 1 << 20
         sc = synth.random_fr(n, 5, 77, device=dev)
         bases = pk.a[:n] if pk.a.shape[0] >= n else synth.fixed_base(1, synth.random_fr(n, 5, 78, device=dev))
-        c = args.window
+        # the width the tuning table gives a 2^20-point table MSM, else the prover's
+        c = autotune.get_value("table_window", 1, 20) or args.window
+        g1_window = c
         W = msm.windows_for(c)
         table = msm.precompute(1, bases, c, W, n)
         ws = torch.empty(msm.workspace_bytes(1, n, c, True, n), dtype=torch.uint8, device=dev)
@@ -757,9 +760,12 @@ def main():
         s16, b16 = sc[:n16], bases[:n16]
         other["g1_msm_2e16_plain_ms"] = timed(lambda: msm.msm(1, s16, b16))
         if pk.b2.shape[0] >= n:
-            t2 = msm.precompute(2, pk.b2[:n], c, W, n)
-            ws2 = torch.empty(msm.workspace_bytes(2, n, c, True, n), dtype=torch.uint8, device=dev)
-            other["g2_msm_2e20_ms"] = timed(lambda: msm.msm_precomputed(2, sc, t2, c, W, n, workspace=ws2))
+            c2 = autotune.get_value("table_window", 2, 20) or args.window
+            W2 = msm.windows_for(c2)
+            t2 = msm.precompute(2, pk.b2[:n], c2, W2, n)
+            ws2 = torch.empty(msm.workspace_bytes(2, n, c2, True, n), dtype=torch.uint8, device=dev)
+            other["g2_msm_2e20_ms"] = timed(lambda: msm.msm_precomputed(2, sc, t2, c2, W2, n, workspace=ws2))
+            other["g2_msm_2e20_window_bits"] = c2
             del t2, ws2
         big = synth.random_fr(1 << 24, 6, 80, device=dev)
         ntt.prepare(24)
@@ -809,7 +815,7 @@ def main():
 
     iso_line = None
     if iso_n:
-        iso_alg = iso_pts * W * FP_MUL_PER_G1_MADD * IMAD_PER_FP_MUL
+        iso_alg = iso_pts * msm.windows_for(g1_window) * FP_MUL_PER_G1_MADD * IMAD_PER_FP_MUL
         iso_avg = iso_ms / iso_n
         iso_line = {"workload": f"G1 MSM 2^{int(np.log2(iso_pts))} alone", "avg_launch_ms": iso_avg,
                     "launches": iso_n, "achieved": iso_alg / (iso_avg * 1e-3) / 1e12,
@@ -846,7 +852,7 @@ def main():
                    "tuning_table": os.path.relpath(tuning, ROOT) if tuning else "built-in defaults"},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                        "mean": float(np.mean(lat))},
-        "g1_msm_2e20_ms": g1_ms, "g1_msm_2e20_plain_ms": g1_plain_ms,
+        "g1_msm_2e20_ms": g1_ms, "g1_msm_2e20_window_bits": g1_window, "g1_msm_2e20_plain_ms": g1_plain_ms,
         "other_configs_ms": other,
         "rooflines_other": rooflines_other,
         "e2e": {"value": world * args.steps / (e2e_ms * 1e-3), "unit": "proofs/s",
