@@ -107,10 +107,11 @@ def tune_msm(group=1, log_ns=range(10, 21), spread=2, reps=3, seed=11, chunks=(3
     return out
 
 
-def tune_msm_table(group=1, log_ns=range(10, 21), spread=2, reps=3, seed=11, runs=(4, 8, 16), chunks=(32, 64, 128)):
+def tune_msm_table(group=1, log_ns=range(10, 21), spread=(4, 2), reps=3, seed=11, runs=(4, 8, 16), chunks=(32, 64, 128)):
     """window width and reduction run (together), then chunk, of an MSM over
     a shifted-copy table, per size class, timing one MSM of 2^log_n points
-    (the table of each width built outside the timing); installs the best
+    (the table of each width built outside the timing; widths from
+    spread[0] below the cost model's to spread[1] above); installs the best
     and returns {log_n: {"window", "run", "chunk", "ms": {"c,run": ms},
     "chunk_ms": {chunk: ms}}}"""
     out = {}
@@ -124,7 +125,9 @@ def tune_msm_table(group=1, log_ns=range(10, 21), spread=2, reps=3, seed=11, run
             set_value(knob, group, lg, 0)
         c0 = msm.autotune_window(group, n, precomputed=True)
         res, tabs = {}, {}
-        for c in range(max(4, c0 - spread), min(20, c0 + spread) + 1):
+        # the model leans to wide windows (it undercounts the bucket
+        # reduction), so the candidates reach further below it than above
+        for c in range(max(4, c0 - spread[0]), min(20, c0 + spread[1]) + 1):
             w = msm.windows_for(c)
             tabs[c] = msm.precompute(group, b, c, w, n)
             for r in runs:
