@@ -16,7 +16,7 @@
 // add-2008-s, dbl-2008-s-1); results are compared with the reference only
 // after normalisation to affine, which is representation independent.
 #pragma once
-#include "field.cuh"
+#include "field52.cuh"
 
 namespace lzk {
 
@@ -101,8 +101,8 @@ static __device__ __noinline__ Fq2 inverse(const Fq2& a)
 
 // Products used by the point formulas: out-of-line Fq products (mul_call),
 // Fq2 products built from them.
-__device__ __forceinline__ Fq cmul(const Fq& a, const Fq& b) { return mul_call(a, b); }
-__device__ __forceinline__ Fq csqr(const Fq& a) { return mul_call(a, a); }
+__device__ __forceinline__ Fq cmul(const Fq& a, const Fq& b) { return mul52_call(a, b); }
+__device__ __forceinline__ Fq csqr(const Fq& a) { return mul52_call(a, a); }
 // One out-of-line body per Fq2 product (and square): its limb products are
 // inlined there, so they interleave, and the call boundary moves two Fq2
 // operands once instead of once per Fq product.
@@ -113,7 +113,7 @@ __device__ __forceinline__ Fq2 csqr(const Fq2& a) { return fq2_sqr_call(a); }
 // two independent products: Fq pairs share one out-of-line body
 __device__ __forceinline__ void cmul2(Fq& r0, Fq& r1, const Fq& a0, const Fq& b0, const Fq& a1, const Fq& b1)
 {
-    FpPair<FqP> r = mul2_call(a0, b0, a1, b1);
+    FpPair<FqP> r = mul52x2_call(a0, b0, a1, b1);
     r0 = r.a;
     r1 = r.b;
 }
