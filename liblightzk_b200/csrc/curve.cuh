@@ -106,8 +106,19 @@ __device__ __forceinline__ Fq csqr(const Fq& a) { return mul52_call(a, a); }
 // One out-of-line body per Fq2 product (and square): its limb products are
 // inlined there, so they interleave, and the call boundary moves two Fq2
 // operands once instead of once per Fq product.
-static __device__ __noinline__ Fq2 fq2_mul_call(const Fq2 a, const Fq2 b) { return mul(a, b); }
-static __device__ __noinline__ Fq2 fq2_sqr_call(const Fq2 a) { return sqr(a); }
+// Both run their Fq products on the FP64 pipe (field52.cuh).
+static __device__ __noinline__ Fq2 fq2_mul_call(const Fq2 a, const Fq2 b)
+{
+    Fq2 r;
+    fq2_mul52(r.c0.v, r.c1.v, a.c0.v, a.c1.v, b.c0.v, b.c1.v);
+    return r;
+}
+static __device__ __noinline__ Fq2 fq2_sqr_call(const Fq2 a)
+{
+    Fq s = add(a.c0, a.c1), d = sub(a.c0, a.c1);
+    Fq x = mul52(s, d), y = mul52(a.c0, a.c1);
+    return {x, dbl(y)};
+}
 __device__ __forceinline__ Fq2 cmul(const Fq2& a, const Fq2& b) { return fq2_mul_call(a, b); }
 __device__ __forceinline__ Fq2 csqr(const Fq2& a) { return fq2_sqr_call(a); }
 // two independent products: Fq pairs share one out-of-line body

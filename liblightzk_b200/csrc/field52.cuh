@@ -152,6 +152,131 @@ __device__ __forceinline__ void mont52_core(uint64_t r[5], const double a[5], co
     r[4] = c[9];
 }
 
+// Bias of the split terms a product a*b leaves in column k (prod_cols52), and
+// of the terms one Montgomery reduction adds to column k (redc52).
+__host__ __device__ constexpr uint64_t prod_bias52(int k)
+{
+    uint64_t b = 0;
+    for (int i = 0; i < 5; i++)
+        for (int j = 0; j < 5; j++) {
+            if (i + j == k) b += kLoBias;
+            if (i + j + 1 == k) b += kHiBias;
+        }
+    return b;
+}
+__host__ __device__ constexpr uint64_t red_bias52(int k)
+{
+    uint64_t b = 0;
+    for (int i = 0; i < 5; i++)
+        for (int j = 0; j < 5; j++) {
+            if (i + j + 1 == k) b += kHiBias;
+            if (j >= 1 && i + j == k) b += kLoBias;
+        }
+    return b;
+}
+
+// c[k] += the split terms of a*b in column k (each term carries its bias)
+__device__ __forceinline__ void prod_cols52(uint64_t c[10], const double a[5], const double b[5])
+{
+    _Pragma("unroll") for (int i = 0; i < 5; i++)
+        _Pragma("unroll") for (int j = 0; j < 5; j++) {
+            uint64_t hi, lo;
+            split52(a[i], b[j], hi, lo);
+            c[i + j] += lo;
+            c[i + j + 1] += hi;
+        }
+}
+
+// Montgomery reduction of an integer given as ten signed 64-bit columns
+// (true values, radix 2^52, total in [0, p * 2^260)): r = total / 2^260 mod p,
+// r < 2p, as normalised limbs.  The columns may be negative individually.
+template <class P>
+__device__ __forceinline__ void redc52(uint64_t r[5], uint64_t c[10])
+{
+    _Pragma("unroll") for (int k = 1; k < 10; k++) c[k] -= red_bias52(k);
+    _Pragma("unroll") for (int i = 0; i < 5; i++) {
+        const double m = u52_to_d((c[i] * P52<P>::ninv) & kM52);
+        c[i + 1] += split52_hi(m, (double)P52<P>::p(0));
+        _Pragma("unroll") for (int j = 1; j < 5; j++) {
+            uint64_t hi, lo;
+            split52(m, (double)P52<P>::p(j), hi, lo);
+            c[i + j] += lo;
+            c[i + j + 1] += hi;
+        }
+        c[i + 1] += (uint64_t)((int64_t)(c[i] + kM52) >> 52);   // ceil(c_i / 2^52)
+    }
+    _Pragma("unroll") for (int k = 5; k < 9; k++) {
+        r[k - 5] = c[k] & kM52;
+        c[k + 1] += (uint64_t)((int64_t)c[k] >> 52);
+    }
+    r[4] = c[9];
+}
+
+// 16 p^2 (Fq) in radix 2^52: keeps a0 b0 - a1 b1 non-negative below
+__host__ __device__ constexpr uint64_t fq_16p2_52(int k)
+{
+    return k == 0 ? 0x58a2275d69b10ull : k == 1 ? 0xd09eac1013b54ull : k == 2 ? 0x96cadca602072ull
+         : k == 3 ? 0x2c84a50189c6dull : k == 4 ? 0x4689e957a124ull : k == 5 ? 0xdfa5c34c6b38dull
+         : k == 6 ? 0x511637560626eull : k == 7 ? 0x348d21cb00b85ull : k == 8 ? 0xbf9c599a6f7c0ull : 0x925c4b8763cull;
+}
+
+// a + b of two 8-limb integers below 2^255 (no reduction)
+__device__ __forceinline__ void add_nored(uint32_t s[8], const uint32_t a[8], const uint32_t b[8])
+{
+    uint32_t c = 0;
+    _Pragma("unroll") for (int k = 0; k < 8; k++) {
+        uint64_t x = (uint64_t)a[k] + b[k] + c;
+        s[k] = (uint32_t)x;
+        c = (uint32_t)(x >> 32);
+    }
+}
+
+// Fq2 product (i^2 = -1) by Karatsuba with lazy reduction, on the FP64 pipe:
+// with one operand scaled by 16 as in mul52,
+//   c0 = 16 (a0 b0 - a1 b1) + 16 p^2  in (0, 32 p^2),
+//   c1 = 16 (a0 + a1)(b0 + b1) - 16 a0 b0 - 16 a1 b1 = 16 (a0 b1 + a1 b0) in [0, 32 p^2),
+// three 5x5-limb products and two reductions (each result < 2p, then one
+// conditional subtraction): the canonical values of the schoolbook product.
+__device__ __forceinline__ void fq2_mul52(uint32_t c0[8], uint32_t c1[8], const uint32_t a0[8], const uint32_t a1[8],
+                                          const uint32_t b0[8], const uint32_t b1[8])
+{
+    uint64_t x[10], y[10];
+    {
+        double da0[5], da1[5], db0[5], db1[5];
+        to_d52<4>(da0, a0);
+        to_d52<4>(da1, a1);
+        to_d52<0>(db0, b0);
+        to_d52<0>(db1, b1);
+        _Pragma("unroll") for (int k = 0; k < 10; k++) { x[k] = 0; y[k] = 0; }
+        prod_cols52(x, da0, db0);
+        prod_cols52(y, da1, db1);
+    }
+    // x = a0 b0 + bias, y = a1 b1 + bias (per column)
+    uint64_t r0[10], r1[10];
+    _Pragma("unroll") for (int k = 0; k < 10; k++) {
+        r0[k] = x[k] - y[k] + fq_16p2_52(k);
+        r1[k] = prod_bias52(k) - x[k] - y[k];
+    }
+    {
+        uint32_t sa[8], sb[8];
+        add_nored(sa, a0, a1);
+        add_nored(sb, b0, b1);
+        double ds[5], dt[5];
+        to_d52<4>(ds, sa);
+        to_d52<0>(dt, sb);
+        prod_cols52(r1, ds, dt);
+    }
+    uint64_t q0[5], q1[5];
+    redc52<FqP>(q0, r0);
+    redc52<FqP>(q1, r1);
+    uint32_t t[8];
+    from_limbs52(t, q0);
+    Fq f0 = final_sub<FqP>(t);
+    from_limbs52(t, q1);
+    Fq f1 = final_sub<FqP>(t);
+    _Pragma("unroll") for (int k = 0; k < 8; k++) { c0[k] = f0.v[k]; c1[k] = f1.v[k]; }
+}
+
 // Drop-in for mul(): canonical 8x32-bit Montgomery operands (R = 2^256),
 // canonical result, the same bits.
 template <class P>

@@ -164,10 +164,11 @@ __device__ __forceinline__ Aff<F> load_base(const void* bases, uint32_t v)
 }
 
 // 128-thread blocks; at most 102 registers for G1 (5 blocks = 20 warps per
-// SM) and 170 for G2 (3 blocks; measured 1.5 % faster than 2 blocks at 250
-// registers despite some spilling, and faster than 4 blocks)
+// SM; 4 and 6 blocks measured the same) and 255 for G2 (2 blocks: with the
+// Fq2 products on the FP64 pipe, 2 blocks measured 10 % faster than 3 and
+// 16 % faster than 4, whose register bounds make the calls spill)
 template <class F, int LAYOUT>
-__global__ void __launch_bounds__(128, sizeof(F) == 32 ? 5 : 3) k_accumulate(const void* __restrict__ bases, const uint32_t* __restrict__ ent,
+__global__ void __launch_bounds__(128, sizeof(F) == 32 ? 5 : 2) k_accumulate(const void* __restrict__ bases, const uint32_t* __restrict__ ent,
                                                     const uint32_t* __restrict__ off, uint32_t B, size_t chunks,
                                                     uint32_t chunk, uint64_t nbases, XYZZ<F>* __restrict__ bsum,
                                                     XYZZ<F>* __restrict__ head, XYZZ<F>* __restrict__ tail)

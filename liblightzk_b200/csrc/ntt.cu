@@ -211,12 +211,12 @@ __global__ void __launch_bounds__(kNttThreads) k_ntt_pass(Fr* __restrict__ data,
             size_t jm = (((size_t)(g & ((1u << hb) - 1))) << p.lowbits) | low;
             Fr lo = ld_elem(sm + i0), hi = ld_elem(sm + i1);
             if (DIT) {
-                Fr u = mul(hi, ldg_elem(tw + (jm << (p.k - 1 - (p.lowbits + t)))));
+                Fr u = mul52(hi, ldg_elem(tw + (jm << (p.k - 1 - (p.lowbits + t)))));
                 st_elem(sm + i0, add(lo, u));
                 st_elem(sm + i1, sub(lo, u));
             } else {
                 st_elem(sm + i0, add(lo, hi));
-                st_elem(sm + i1, mul(sub(lo, hi), ldg_elem(tw + (jm << (p.s0 + t)))));
+                st_elem(sm + i1, mul52(sub(lo, hi), ldg_elem(tw + (jm << (p.s0 + t)))));
             }
         }
         __syncthreads();

@@ -1,7 +1,7 @@
 // ntt.cuh -- internal interface of the NTT (ntt.cu) for other operators.
 #pragma once
 #include "common.cuh"
-#include "field.cuh"
+#include "field52.cuh"
 
 namespace lzk {
 
