@@ -785,10 +785,12 @@ def main():
     # ---------------- roofline of the dominant kernel ----------------
     mad_chain_rate = _capi.probe_imad_rate()
     mont_rate = _capi.probe_mont_rate()
+    mont_rate_int = _capi.probe_mont_rate_int()
     # the roofline's denominator: Montgomery products per second in the
-    # kernels' own instruction form, counted in the IMAD-class unit of the
+    # fastest product form measured on this GPU (the FP64-pipe product with
+    # operands kept as limbs), counted in the IMAD-class unit of the
     # algorithmic work (264 per product)
-    imad_peak = mont_rate * IMAD_PER_FP_MUL
+    imad_peak = max(mont_rate, mont_rate_int) * IMAD_PER_FP_MUL
     W = msm.windows_for(args.window)
     nl = circ.n_vars - circ.n_public - 1
     # G1 accumulation launches per proof: A, B1, and L + H as one MSM
@@ -798,7 +800,7 @@ def main():
     alg_imad = avg_pts * W * FP_MUL_PER_G1_MADD * IMAD_PER_FP_MUL
     acc_avg_ms = acc_ms / max(acc_n, 1)
     achieved = alg_imad / (acc_avg_ms * 1e-3) if acc_n else None
-    traffic = pipe_util = pipe_util_probe = None
+    traffic = pipe_util = pipe_util_probe = pipe_name = None
     prof = os.path.join(ROOT, "profiles", "msm_g1_accumulate_traffic.json")
     if os.path.exists(prof):
         try:
@@ -806,12 +808,14 @@ def main():
             # per average launch of this proof, scaled by its points from the
             # captured launch (traffic grows with the entries)
             traffic = tj["bytes_per_launch_at_2e20"] * avg_pts / tj["points_at_2e20"]
-            # ncu's multiplier (fmaheavy) pipe activity of that launch, and of
-            # the product probe that sets `peak`
-            pipe_util = tj["fmaheavy_pipe_active_pct"] / 100.0
-            pipe_util_probe = tj["fmaheavy_pipe_active_pct_probe"] / 100.0
+            # ncu's activity of the pipe that binds the products (FP64) in
+            # that launch and in the product probe that sets `peak`
+            if tj.get("pipe_active_pct") is not None:
+                pipe_name = tj["pipe"]
+                pipe_util = tj["pipe_active_pct"] / 100.0
+                pipe_util_probe = tj["pipe_active_pct_probe"] / 100.0
         except Exception:
-            traffic = pipe_util = pipe_util_probe = None
+            traffic = pipe_util = pipe_util_probe = pipe_name = None
 
     iso_line = None
     if iso_n:
@@ -869,11 +873,12 @@ def main():
                      "achieved": iso_line["achieved"] if iso_line else None, "peak": imad_peak / 1e12,
                      "unit": "T IMAD/s", "frac": iso_line["frac"] if iso_line else None,
                      "traffic": iso_line["traffic_bytes"] if iso_line else None,
-                     "peak_source": "measured: lzk_probe_mont_rate (independent Fq Montgomery products in the "
-                                    "kernels' instruction form, full occupancy) x 264 IMAD-class per product",
-                     "mont_products_per_s": mont_rate,
-                     "pipe_util": pipe_util, "pipe_util_probe": pipe_util_probe,
-                     "pipe_util_source": "ncu sm__pipe_fmaheavy_cycles_active of one G1 accumulation launch at 2^20 "
+                     "peak_source": "measured: lzk_probe_mont_rate (independent Fq Montgomery products on the "
+                                    "FP64 pipe, operands kept as radix-2^52 limbs, full occupancy; the faster of "
+                                    "it and the 32-bit-limb integer form) x 264 IMAD-class per product",
+                     "mont_products_per_s": mont_rate, "mont_products_per_s_int_form": mont_rate_int,
+                     "pipe": pipe_name, "pipe_util": pipe_util, "pipe_util_probe": pipe_util_probe,
+                     "pipe_util_source": "ncu sm__pipe_fp64_cycles_active of one G1 accumulation launch at 2^20 "
                                          "and of the probe (profiles/k_accumulate_2e20.md)",
                      "peak_mad_chains_T": mad_chain_rate / 1e12,
                      "algorithmic_imad_per_launch": iso_line["algorithmic_imad_per_launch"] if iso_line else None,

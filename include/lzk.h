@@ -537,10 +537,14 @@ uint64_t lzk_launch_count(void);
 /* Measured 32-bit integer multiply-add rate of the current device
  * (mad.lo/madc.hi operations per second); synchronous. */
 int lzk_probe_imad_rate(double* ops_per_s);
-/* Measured rate of Fq Montgomery products per second on the current device,
- * in the instruction form the MSM and NTT kernels issue (independent
- * products, full occupancy); synchronous. */
+/* Measured rate of Fq Montgomery products per second on the current device
+ * in the fastest form this library has: the radix-2^52 product on the FP64
+ * pipe with operands already in limb form (independent products, full
+ * occupancy); synchronous. */
 int lzk_probe_mont_rate(double* products_per_s);
+/* The same for the 32-bit-limb integer product (wide multiplies on the
+ * integer multiplier); synchronous. */
+int lzk_probe_mont_rate_int(double* products_per_s);
 
 #ifdef __cplusplus
 }

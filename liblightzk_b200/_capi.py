@@ -76,6 +76,7 @@ SIGNATURES = {
     "lzk_trace_timeline": (c_i, [c_p, c_sz, ctypes.POINTER(c_sz)]),
     "lzk_probe_imad_rate": (c_i, [ctypes.POINTER(ctypes.c_double)]),
     "lzk_probe_mont_rate": (c_i, [ctypes.POINTER(ctypes.c_double)]),
+    "lzk_probe_mont_rate_int": (c_i, [ctypes.POINTER(ctypes.c_double)]),
     "lzk_launch_count": (ctypes.c_uint64, []),
     "lzk_debug_fail_allocations": (c_i, [ctypes.c_longlong]),
     "lzk_debug_check_word": (c_u32, [c_i]),
@@ -211,6 +212,12 @@ def probe_imad_rate():
 def probe_mont_rate():
     r = ctypes.c_double()
     call("lzk_probe_mont_rate", ctypes.byref(r))
+    return r.value
+
+
+def probe_mont_rate_int():
+    r = ctypes.c_double()
+    call("lzk_probe_mont_rate_int", ctypes.byref(r))
     return r.value
 
 

@@ -163,12 +163,13 @@ __device__ __forceinline__ Aff<F> load_base(const void* bases, uint32_t v)
     return p;
 }
 
-// 128-thread blocks; at most 102 registers for G1 (5 blocks = 20 warps per
-// SM; 4 and 6 blocks measured the same) and 255 for G2 (2 blocks: with the
-// Fq2 products on the FP64 pipe, 2 blocks measured 10 % faster than 3 and
-// 16 % faster than 4, whose register bounds make the calls spill)
+// 128-thread blocks; at most 168 registers for G1 (3 blocks = 12 warps per
+// SM) and 255 for G2 (2 blocks).  With the products on the FP64 pipe the
+// tighter register bounds make the product calls spill: G1 at 3 blocks/SM
+// measured 6 % faster than at 5 (which matched 4 and 6), G2 at 2 blocks 10 %
+// faster than at 3 and 16 % faster than at 4.
 template <class F, int LAYOUT>
-__global__ void __launch_bounds__(128, sizeof(F) == 32 ? 5 : 2) k_accumulate(const void* __restrict__ bases, const uint32_t* __restrict__ ent,
+__global__ void __launch_bounds__(128, sizeof(F) == 32 ? 3 : 2) k_accumulate(const void* __restrict__ bases, const uint32_t* __restrict__ ent,
                                                     const uint32_t* __restrict__ off, uint32_t B, size_t chunks,
                                                     uint32_t chunk, uint64_t nbases, XYZZ<F>* __restrict__ bsum,
                                                     XYZZ<F>* __restrict__ head, XYZZ<F>* __restrict__ tail)

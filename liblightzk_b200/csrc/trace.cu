@@ -6,7 +6,7 @@
 // every phase; here a traced region only records two events on its stream,
 // and durations are resolved when the host asks for them.
 #include "common.cuh"
-#include "field.cuh"
+#include "field52.cuh"
 #include <nvtx3/nvToolsExt.h>
 #include <atomic>
 #include <map>
@@ -135,13 +135,15 @@ __global__ void k_imad_probe(uint32_t iters, uint32_t seed, uint32_t* sink)
     if (acc == 0x12345678u) sink[0] = acc;
 }
 
-// Independent Montgomery products in the form the MSM and NTT kernels issue
-// (mul: mont_mul_core's wide products and 64-bit additions, then the final
-// conditional subtraction): each thread keeps kMontChains products in
-// flight, x_k <- x_k * y, so the rate is bound by the product's
-// instructions, not by a dependency chain.
+// Independent Montgomery products, x_k <- x_k * y with kMontChains products
+// in flight per thread, so the rate is bound by the product's instructions,
+// not by a dependency chain.  FP: the radix-2^52 product on the FP64 pipe
+// (mont52_core, operands kept as limbs between products: the fastest form
+// this library has, the roofline's denominator); INT: the 32-bit-limb
+// product (mul: wide integer multiplies, then the conditional subtraction).
 constexpr int kMontChains = 4;
-__global__ void __launch_bounds__(128) k_mont_probe(uint32_t iters, uint32_t seed, uint32_t* sink)
+template <bool FP>
+__device__ __forceinline__ void mont_probe_body(uint32_t iters, uint32_t seed, uint32_t* sink)
 {
     Fq x[kMontChains], y;
     uint32_t h = seed * 0x9e3779b9u ^ (uint32_t)gtid();
@@ -152,14 +154,71 @@ __global__ void __launch_bounds__(128) k_mont_probe(uint32_t iters, uint32_t see
     }
     y.v[7] &= 0x0fffffffu;                       // operands below p
     for (int k = 0; k < kMontChains; k++) x[k].v[7] &= 0x0fffffffu;
-    for (uint32_t it = 0; it < iters; it++) {
-        #pragma unroll
-        for (int k = 0; k < kMontChains; k++) x[k] = mul(x[k], y);
-    }
     uint32_t acc = 0;
-    for (int k = 0; k < kMontChains; k++)
-        for (int i = 0; i < 8; i++) acc ^= x[k].v[i];
+    if (FP) {
+        double dx[kMontChains][5], dy[5];
+        to_d52<0>(dy, y.v);
+        for (int k = 0; k < kMontChains; k++) to_d52<0>(dx[k], x[k].v);
+        for (uint32_t it = 0; it < iters; it++) {
+            #pragma unroll
+            for (int k = 0; k < kMontChains; k++) {
+                uint64_t r[5];
+                mont52_core<FqP>(r, dx[k], dy);
+                #pragma unroll
+                for (int i = 0; i < 5; i++) dx[k][i] = u52_to_d(r[i]);   // r < 2p: limbs < 2^52
+            }
+        }
+        for (int k = 0; k < kMontChains; k++)
+            for (int i = 0; i < 5; i++) acc ^= (uint32_t)__double_as_longlong(dx[k][i]);
+    } else {
+        for (uint32_t it = 0; it < iters; it++) {
+            #pragma unroll
+            for (int k = 0; k < kMontChains; k++) x[k] = mul(x[k], y);
+        }
+        for (int k = 0; k < kMontChains; k++)
+            for (int i = 0; i < 8; i++) acc ^= x[k].v[i];
+    }
     if (acc == 0x12345678u) sink[0] = acc;
+}
+__global__ void __launch_bounds__(128) k_mont_probe_int(uint32_t iters, uint32_t seed, uint32_t* sink)
+{
+    mont_probe_body<false>(iters, seed, sink);
+}
+__global__ void __launch_bounds__(128, 2) k_mont_probe_fp(uint32_t iters, uint32_t seed, uint32_t* sink)
+{
+    mont_probe_body<true>(iters, seed, sink);
+}
+
+// Measured rate of Fq Montgomery products on this device at full
+// occupancy, in the FP64 form (fp) or the 32-bit-limb form.  Synchronous;
+// ~0.1 s.
+template <bool FP>
+static int probe_mont(double* products_per_s)
+{
+    if (!products_per_s) return LZK_EINVAL;
+    int per_sm = 0;
+    auto kern = FP ? k_mont_probe_fp : k_mont_probe_int;
+    LZK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, 0));
+    if (per_sm <= 0) return LZK_EDEVICE;
+    uint32_t* sink;
+    LZK_CUDA(cudaMalloc(&sink, 4));
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const uint32_t iters = 2048, threads = 128, blocks = sm_count() * (uint32_t)per_sm * 4;
+    kern<<<blocks, threads>>>(16, 1u, sink); note_launch();  // warm-up
+    cudaEventRecord(a);
+    kern<<<blocks, threads>>>(iters, 1u, sink); note_launch();
+    cudaEventRecord(b);
+    cudaError_t e = cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(sink);
+    if (e != cudaSuccess) return cuda_status(e);
+    *products_per_s = (double)blocks * threads * iters * kMontChains / (ms * 1e-3);
+    return LZK_OK;
 }
 
 }  // namespace lzk
@@ -264,33 +323,7 @@ int lzk_probe_imad_rate(double* ops_per_s)
     return LZK_OK;
 }
 
-// Measured rate of Montgomery products (Fq, the instruction form of the
-// kernels' products) on this device at full occupancy.  Synchronous; ~0.1 s.
-int lzk_probe_mont_rate(double* products_per_s)
-{
-    if (!products_per_s) return LZK_EINVAL;
-    int per_sm = 0;
-    LZK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mont_probe, 128, 0));
-    if (per_sm <= 0) return LZK_EDEVICE;
-    uint32_t* sink;
-    LZK_CUDA(cudaMalloc(&sink, 4));
-    cudaEvent_t a, b;
-    cudaEventCreate(&a);
-    cudaEventCreate(&b);
-    const uint32_t iters = 2048, threads = 128, blocks = sm_count() * (uint32_t)per_sm * 4;
-    k_mont_probe<<<blocks, threads>>>(16, 1u, sink); note_launch();  // warm-up
-    cudaEventRecord(a);
-    k_mont_probe<<<blocks, threads>>>(iters, 1u, sink); note_launch();
-    cudaEventRecord(b);
-    cudaError_t e = cudaEventSynchronize(b);
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, a, b);
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
-    cudaFree(sink);
-    if (e != cudaSuccess) return cuda_status(e);
-    *products_per_s = (double)blocks * threads * iters * kMontChains / (ms * 1e-3);
-    return LZK_OK;
-}
+int lzk_probe_mont_rate(double* products_per_s) { return probe_mont<true>(products_per_s); }
+int lzk_probe_mont_rate_int(double* products_per_s) { return probe_mont<false>(products_per_s); }
 
 }  // extern "C"
