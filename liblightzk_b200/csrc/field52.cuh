@@ -277,6 +277,56 @@ __device__ __forceinline__ void fq2_mul52(uint32_t c0[8], uint32_t c1[8], const 
     _Pragma("unroll") for (int k = 0; k < 8; k++) { c0[k] = f0.v[k]; c1[k] = f1.v[k]; }
 }
 
+// Montgomery square r = a^2 / 2^260 mod p (r < 2p) for limbs a < 2^52 with
+// a^2 < p * 2^260: 15 limb products instead of 25, the cross products'
+// halves added twice.
+__host__ __device__ constexpr uint64_t sq_bias52(int k)
+{
+    uint64_t b = 0;
+    for (int i = 0; i < 5; i++) {
+        if (2 * i == k) b += kLoBias;
+        if (2 * i + 1 == k) b += kHiBias;
+        for (int j = i + 1; j < 5; j++) {
+            if (i + j == k) b += 2 * kLoBias;
+            if (i + j + 1 == k) b += 2 * kHiBias;
+        }
+    }
+    return b;
+}
+template <class P>
+__device__ __forceinline__ void mont52_sqr_core(uint64_t r[5], const double a[5])
+{
+    uint64_t c[10];
+    _Pragma("unroll") for (int k = 0; k < 10; k++) c[k] = 0 - sq_bias52(k) - red_bias52(k);
+    _Pragma("unroll") for (int i = 0; i < 5; i++) {
+        uint64_t hi, lo;
+        split52(a[i], a[i], hi, lo);
+        c[2 * i] += lo;
+        c[2 * i + 1] += hi;
+        _Pragma("unroll") for (int j = i + 1; j < 5; j++) {
+            split52(a[i], a[j], hi, lo);
+            c[i + j] = c[i + j] + lo + lo;
+            c[i + j + 1] = c[i + j + 1] + hi + hi;
+        }
+    }
+    _Pragma("unroll") for (int i = 0; i < 5; i++) {
+        const double m = u52_to_d((c[i] * P52<P>::ninv) & kM52);
+        c[i + 1] += split52_hi(m, (double)P52<P>::p(0));
+        _Pragma("unroll") for (int j = 1; j < 5; j++) {
+            uint64_t hi, lo;
+            split52(m, (double)P52<P>::p(j), hi, lo);
+            c[i + j] += lo;
+            c[i + j + 1] += hi;
+        }
+        c[i + 1] += (c[i] + kM52) >> 52;
+    }
+    _Pragma("unroll") for (int k = 5; k < 9; k++) {
+        r[k - 5] = c[k] & kM52;
+        c[k + 1] += c[k] >> 52;
+    }
+    r[4] = c[9];
+}
+
 // Drop-in for mul(): canonical 8x32-bit Montgomery operands (R = 2^256),
 // canonical result, the same bits.
 template <class P>
@@ -292,13 +342,33 @@ __device__ __forceinline__ Fp<P> mul52(const Fp<P>& a, const Fp<P>& b)
     return final_sub<P>(t);
 }
 
-// Out-of-line bodies for the curve formulas (one product, or two independent
-// products interleaved), as mul_call / mul2_call in field.cuh.
+// Square with the drop-in interface: the operand enters as 4a, so
+// (4a)^2 / 2^260 = a^2 / 2^256, from 15 limb products instead of 25.
+template <class P>
+__device__ __forceinline__ Fp<P> sqr52(const Fp<P>& a)
+{
+    double da[5];
+    to_d52<2>(da, a.v);
+    uint64_t r[5];
+    mont52_sqr_core<P>(r, da);
+    uint32_t t[8];
+    from_limbs52(t, r);
+    return final_sub<P>(t);
+}
+
+// Out-of-line bodies for the curve formulas (one product, two independent
+// products interleaved, or two squares), as mul_call / mul2_call in
+// field.cuh.
 template <class P> __device__ __noinline__ Fp<P> mul52_call(const Fp<P> a, const Fp<P> b) { return mul52(a, b); }
 template <class P>
 __device__ __noinline__ FpPair<P> mul52x2_call(const Fp<P> a0, const Fp<P> b0, const Fp<P> a1, const Fp<P> b1)
 {
     return FpPair<P>{mul52(a0, b0), mul52(a1, b1)};
+}
+template <class P>
+__device__ __noinline__ FpPair<P> sqr52x2_call(const Fp<P> a, const Fp<P> b)
+{
+    return FpPair<P>{sqr52(a), sqr52(b)};
 }
 
 }  // namespace lzk
