@@ -294,6 +294,7 @@ def run_batch_case(args):
     msms, ntts, _pool = batch.workload_config3()
     plan = batch.BatchPlan(1, msms, ntts)
     plan_fx = batch.BatchPlan(1, msms, ntts, fixed_bases=True)
+    plan_px = batch.BatchPlan(1, msms, ntts, fixed_bases=True, persistent=True)
     stream = torch.cuda.Stream()
     torch.cuda.synchronize()
 
@@ -313,6 +314,9 @@ def run_batch_case(args):
     torch.cuda.synchronize()
     plan_ms = timed(lambda: plan.run(use_graph=True, stream=stream), args.reps)
     plan_fx_ms = timed(lambda: plan_fx.run(use_graph=True, stream=stream), args.reps)
+    # the MSM phases after the sort as one persistent launch (eager, synchronous runs)
+    plan_px.run(stream=stream)
+    plan_px_ms = timed(lambda: plan_px.run(stream=stream), args.reps)
 
     def one_by_one():
         for s, b, o in msms:
@@ -350,21 +354,25 @@ def run_batch_case(args):
         torch.cuda.synchronize()
         _capi.trace_enable(False)
         return {ph: _capi.trace_get(f"batch_{ph}")[0] for ph in ("msm_sort", "msm_accumulate", "msm_fixup",
-                                                                  "msm_reduce", "msm_finish", "ntt")}
+                                                                  "msm_reduce", "msm_finish", "msm_persistent",
+                                                                  "ntt")}
 
-    phases, phases_fx = phases_of(plan), phases_of(plan_fx)
+    phases, phases_fx, phases_px = phases_of(plan), phases_of(plan_fx), phases_of(plan_px)
     pts = sum(int(m[0].shape[0]) for m in msms)
     elems = sum(1 << k for _, k, _ in ntts)
     med = lambda x: float(np.median(x))  # noqa: E731
     print(json.dumps({"case": "batch", "msms": len(msms), "ntts": len(ntts), "msm_points": pts,
                       "ntt_elements": elems,
                       "plan_fixed_bases_graph_ms": plan_fx_ms, "plan_graph_ms": plan_ms,
+                      "plan_fixed_bases_persistent_ms": plan_px_ms,
+                      "speedup_persistent": med(seq_ms) / med(plan_px_ms),
                       "one_by_one_ms": seq_ms, "one_by_one_tables_ms": seq_tab_ms,
                       "speedup": med(seq_ms) / med(plan_fx_ms),
                       "speedup_vs_one_by_one_tables": med(seq_tab_ms) / med(plan_fx_ms),
                       "speedup_plain_plan": med(seq_ms) / med(plan_ms),
                       "plan_device_bytes": plan.device_bytes(), "plan_fixed_bases_device_bytes": plan_fx.device_bytes(),
                       "phases_ms_eager": phases, "phases_ms_eager_fixed_bases": phases_fx,
+                      "phases_ms_persistent": phases_px,
                       "tuning_table": table_src,
                       "tuned": {"msm_g1": {lg: {k: autotune.get_value(k, 1, lg)
                                                 for k in ("window", "run", "chunk", "table_window", "table_run",

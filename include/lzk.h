@@ -434,6 +434,15 @@ int lzk_batch_plan_create(int group, const lzk_msm_desc* msms, size_t n_msm, con
  * every run).  For bases that stay fixed, such as a proving key's queries.
  * Window widths come from LZK_TUNE_MSM_TABLE_WINDOW. */
 #define LZK_BATCH_FIXED_BASES 0x1u
+/* LZK_BATCH_PERSISTENT: the MSM phases after the digit sort (accumulation,
+ * fix-up, the bucket reductions of every window width, the window
+ * combination) run as one cooperative persistent launch of exactly the
+ * blocks the device holds at once, with a grid-wide barrier between phases,
+ * instead of nine launches.  Its barrier waits are bounded (about 2 s; then
+ * LZK_ETIMEOUT).  Runs are eager and synchronous (use_graph is ignored); at
+ * most 20 distinct window widths (else LZK_EUNSUPPORTED at creation).  The
+ * NTTs still run on a second stream beside it. */
+#define LZK_BATCH_PERSISTENT 0x2u
 int lzk_batch_plan_create_ex(int group, const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_desc* ntts,
                              size_t n_ntt, uint32_t flags, lzk_batch_plan** out);
 int lzk_batch_plan_run(lzk_batch_plan* plan, int use_graph, void* stream);

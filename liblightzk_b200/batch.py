@@ -17,12 +17,15 @@ from .device import ptr, stream_ptr
 
 
 FIXED_BASES = 0x1
+PERSISTENT = 0x2
 
 
 class BatchPlan:
-    def __init__(self, group, msms=(), ntts=(), fixed_bases=False):
+    def __init__(self, group, msms=(), ntts=(), fixed_bases=False, persistent=False):
         """fixed_bases: build the MSMs' shifted-copy tables now (the bases are
-        not read again; see LZK_BATCH_FIXED_BASES)"""
+        not read again; see LZK_BATCH_FIXED_BASES); persistent: the MSM phases
+        after the digit sort as one persistent launch (LZK_BATCH_PERSISTENT;
+        runs are then synchronous and never captured)"""
         self.group = group
         self._keep = (list(msms), list(ntts))
         md = (_capi.MsmDesc * max(len(msms), 1))()
@@ -35,7 +38,8 @@ class BatchPlan:
             nd[i].data, nd[i].log_n, nd[i].direction = ptr(d), k, direction
         h = ctypes.c_void_p()
         _capi.call("lzk_batch_plan_create_ex", group, md if msms else None, len(msms), nd if ntts else None,
-                   len(ntts), FIXED_BASES if fixed_bases else 0, ctypes.byref(h))
+                   len(ntts), (FIXED_BASES if fixed_bases else 0) | (PERSISTENT if persistent else 0),
+                   ctypes.byref(h))
         self.handle = h
 
     def run(self, use_graph=False, stream=None):

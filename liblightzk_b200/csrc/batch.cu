@@ -7,7 +7,8 @@
 //   gather bases -> digit count -> offset scan -> scatter -> accumulate
 //   -> fix-up -> bucket reduction (one level chain per window width) ->
 //   window combination (one warp per MSM)
-// so 64 MSMs cost about the launches of one.  MSMs are ordered by window
+// so 64 MSMs cost about the launches of one; with LZK_BATCH_PERSISTENT
+// everything after the scatter is one persistent launch (below).  MSMs are ordered by window
 // width so that the windows of equal width are contiguous and reduce
 // together.  NTTs are grouped by (size, direction) and each group is one
 // set of pass launches over a device table of pointers, on a second stream
@@ -37,6 +38,7 @@ struct lzk_batch_plan {
     int group = 1;
     uint32_t flags = 0;                // LZK_BATCH_*
     bool fixed = false;                // LZK_BATCH_FIXED_BASES: shifted-copy tables built at creation
+    bool persistent = false;           // LZK_BATCH_PERSISTENT: the MSM phases after the sort in one launch
     void* table = nullptr;             // their entries, all MSMs, table_pts points
     uint64_t table_pts = 0;
     size_t table_bytes = 0;
@@ -53,6 +55,7 @@ struct lzk_batch_plan {
     BDesc* d_desc = nullptr;
     uint64_t* d_ptsoff = nullptr;
     uint32_t *cnt = nullptr, *off = nullptr, *ent = nullptr, *bsums = nullptr, *large = nullptr;
+    uint32_t* bar = nullptr;           // persistent launch: barrier count, error word
     void *bases = nullptr, *bsum = nullptr, *head = nullptr, *tail = nullptr, *lr[2] = {nullptr, nullptr},
          *la[2] = {nullptr, nullptr}, *wres = nullptr;
     cudaStream_t s_ntt = nullptr;
@@ -130,10 +133,8 @@ __global__ void k_bdigits(const BDesc* __restrict__ d, const uint64_t* __restric
 // warp-uniform point operations, so the chain of about W * c doublings costs
 // one product per stage instead of a whole serial formula
 template <class F>
-__global__ void k_bfinish(const BDesc* __restrict__ d, uint32_t count, const XYZZ<F>* __restrict__ wres)
+__device__ __forceinline__ void bfinish_one(const BDesc* __restrict__ d, uint32_t k, const XYZZ<F>* __restrict__ wres)
 {
-    const uint32_t k = blockIdx.x;
-    if (k >= count || threadIdx.x >= 32) return;
     const BDesc& m = d[k];
     XYZZ<F> r = xyzz_inf<F>();
     if (m.n) {
@@ -144,7 +145,150 @@ __global__ void k_bfinish(const BDesc* __restrict__ d, uint32_t count, const XYZ
         }
     }
     Jac<F> j = xyzz_to_jac_warp(r);
-    if (threadIdx.x == 0) st_elem(reinterpret_cast<Jac<F>*>(m.out), j);
+    if ((threadIdx.x & 31) == 0) st_elem(reinterpret_cast<Jac<F>*>(m.out), j);
+}
+template <class F>
+__global__ void k_bfinish(const BDesc* __restrict__ d, uint32_t count, const XYZZ<F>* __restrict__ wres)
+{
+    const uint32_t k = blockIdx.x;
+    if (k >= count || threadIdx.x >= 32) return;
+    bfinish_one<F>(d, k, wres);
+}
+
+// ---------------- persistent form (LZK_BATCH_PERSISTENT) ----------------
+// The MSM phases after the digit sort -- accumulation, fix-up, the large
+// buckets' fix-up, the four bucket-reduction steps and the window
+// combination -- as one cooperative launch of exactly the blocks the device
+// holds at once, each phase a grid-stride loop over its items (the bodies of
+// the separate kernels), a grid-wide barrier between phases.  Barrier k
+// waits for k * gridDim.x arrivals on bar[0]; a wait gives up after
+// kBarPolls polls (about 2 s), sets bar[1] and returns false, and every
+// block then leaves at its next barrier, so the kernel always ends; the
+// host reads bar[1] after the run (LZK_ETIMEOUT).
+constexpr uint32_t kBarPolls = 1u << 23;
+
+__device__ __forceinline__ bool persist_barrier(uint32_t* bar, uint32_t phase)
+{
+    __shared__ uint32_t ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(bar, 1u);
+        const uint32_t target = phase * gridDim.x;
+        uint32_t good = 1;
+        for (uint32_t polls = 0;; polls++) {
+            uint32_t v;
+            asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
+            if (v >= target) break;
+            if (*(volatile uint32_t*)(bar + 1)) { good = 0; break; }
+            if (polls >= kBarPolls) { atomicOr(bar + 1, 1u); good = 0; break; }
+            __nanosleep(256);
+        }
+        __threadfence();
+        ok = good;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+template <class F>
+struct PersistArgs {
+    const void* bases;
+    const uint32_t* ent;
+    const uint32_t* off;
+    uint32_t B, chunk;
+    uint64_t chunks, nbases;
+    XYZZ<F> *bsum, *head, *tail;
+    uint32_t* large;
+    uint32_t* bar;
+    uint64_t tiles, nps, nss, sets;    // reduction items (as reduce_jobs counts them)
+    const BDesc* desc;
+    uint32_t count;                    // MSMs
+    const XYZZ<F>* wres;
+};
+
+template <class F>
+__global__ void __launch_bounds__(128, sizeof(F) == 32 ? 3 : 2)
+k_bpersist(const __grid_constant__ PersistArgs<F> a, const __grid_constant__ RedJobs<F> jobs)
+{
+    __shared__ uint4 fx_raw[128 * sizeof(XYZZ<F>) / 16];
+    for (uint64_t t = gtid(); t < a.chunks; t += gstride())
+        accumulate_chunk<F, LZK_BASES_AFFINE>(t, a.bases, a.ent, a.off, a.B, a.chunks, a.chunk, a.nbases, a.bsum,
+                                             a.head, a.tail);
+    if (!persist_barrier(a.bar, 1)) return;
+    fixup_items<F>(a.off, a.B, a.chunk, a.chunks, a.bsum, a.head, a.tail, a.large);
+    if (!persist_barrier(a.bar, 2)) return;
+    fixup_large_items<F>(a.off, a.chunk, a.bsum, a.head, a.tail, a.large, reinterpret_cast<XYZZ<F>*>(fx_raw));
+    if (!persist_barrier(a.bar, 3)) return;
+    red_tile_items<F>(jobs, a.tiles);
+    if (!persist_barrier(a.bar, 4)) return;
+    red_slices_items<F>(jobs, a.nps);
+    if (!persist_barrier(a.bar, 5)) return;
+    red_scale_items<F>(jobs, a.nss);
+    if (!persist_barrier(a.bar, 6)) return;
+    red_combine_items<F>(jobs, a.sets);
+    if (!persist_barrier(a.bar, 7)) return;
+    for (uint64_t k = gtid() >> 5; k < a.count; k += gstride() >> 5) bfinish_one<F>(a.desc, (uint32_t)k, a.wres);
+}
+
+// the reduction jobs of a plan, one per window width, laid out as
+// reduce_jobs lays them (at most kMaxRedJobs: checked at creation)
+template <class F>
+static RedJobs<F> plan_jobs(lzk_batch_plan* p, uint64_t& tiles, uint64_t& nps, uint64_t& nss, uint64_t& sets)
+{
+    using X = XYZZ<F>;
+    RedJobs<F> jobs{};
+    tiles = nps = nss = sets = 0;
+    uint64_t wdone = 0;
+    X* bsum = static_cast<X*>(p->bsum);
+    for (auto& wg : p->wgroups) {
+        const uint64_t o = wg.scratch_off;
+        RedJob<F> j = red_job<F>(bsum + wg.bucket_base, p->off + wg.bucket_base, (uint32_t)wg.windows,
+                                 1u << (wg.c - 1), wg.run, static_cast<X*>(p->lr[0]) + o,
+                                 static_cast<X*>(p->la[0]) + o, static_cast<X*>(p->lr[1]) + o,
+                                 static_cast<X*>(p->la[1]) + o, static_cast<X*>(p->wres) + wdone);
+        wdone += wg.windows;
+        j.s_tile = tiles; j.s_np = nps; j.s_ns = nss; j.s_w = sets;
+        tiles += (uint64_t)j.wb * j.sh.P;
+        nps += (uint64_t)j.wb * j.sh.NP;
+        nss += (uint64_t)j.wb * j.sh.NS;
+        sets += j.wb;
+        jobs.g[jobs.count++] = j;
+    }
+    return jobs;
+}
+
+template <class F>
+static int run_persistent(lzk_batch_plan* p, cudaStream_t st)
+{
+    using X = XYZZ<F>;
+    PersistArgs<F> a{};
+    a.bases = p->fixed ? p->table : p->bases;
+    a.ent = p->ent;
+    a.off = p->off;
+    a.B = (uint32_t)p->total_buckets;
+    a.chunk = p->chunk;
+    a.chunks = p->chunks;
+    a.nbases = p->fixed ? p->table_pts : p->total_pts;
+    a.bsum = static_cast<X*>(p->bsum);
+    a.head = static_cast<X*>(p->head);
+    a.tail = static_cast<X*>(p->tail);
+    a.large = p->large;
+    a.bar = p->bar;
+    a.desc = p->d_desc;
+    a.count = (uint32_t)p->msm.size();
+    a.wres = static_cast<const X*>(p->wres);
+    RedJobs<F> jobs = plan_jobs<F>(p, a.tiles, a.nps, a.nss, a.sets);
+    int per_sm = 0;
+    LZK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bpersist<F>, 128, 0));
+    if (per_sm <= 0) return LZK_EUNSUPPORTED;
+    LZK_CUDA(cudaMemsetAsync(p->large, 0, sizeof(uint32_t), st));
+    LZK_CUDA(cudaMemsetAsync(p->bar, 0, 2 * sizeof(uint32_t), st));
+    void* args[] = {&a, &jobs};
+    LZK_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_bpersist<F>), dim3(sm_count() * per_sm),
+                                         dim3(128), args, 0, st));
+    note_launch();
+    return launch_status();
 }
 
 template <class F>
@@ -163,6 +307,12 @@ static int run_plan(lzk_batch_plan* p, cudaStream_t st)
         LZK_TRY(scan_offsets(p->cnt, (uint32_t)p->total_buckets, p->off, p->bsums, st));
         k_bdigits<true><<<g, 256, 0, st>>>(p->d_desc, p->d_ptsoff, count, p->total_pts, p->fixed, p->off, p->cnt, p->ent); note_launch();
         trace_end(tr, st);
+        if (p->persistent) {
+            tr = trace_begin("batch_msm_persistent", st);
+            LZK_TRY(run_persistent<F>(p, st));
+            trace_end(tr, st);
+            return LZK_OK;
+        }
         X* bsum = static_cast<X*>(p->bsum);
         tr = trace_begin("batch_msm_accumulate", st);
         k_accumulate<F, LZK_BASES_AFFINE><<<grid_for(p->chunks, 128), 128, 0, st>>>(
@@ -193,7 +343,7 @@ static int run_plan(lzk_batch_plan* p, cudaStream_t st)
         LZK_TRY(reduce_jobs<F>(jobs.data(), jobs.size(), st));
         trace_end(tr, st);
     }
-    if (count) {
+    if (count && !(p->persistent && p->total_pts)) {
         void* tr = trace_begin("batch_msm_finish", st);
         k_bfinish<F><<<count, 32, 0, st>>>(p->d_desc, count, static_cast<const X*>(p->wres)); note_launch();
         trace_end(tr, st);
@@ -285,6 +435,8 @@ static int create_plan(const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_des
     // each width group reduces with the run of its own largest MSM's size class
     for (auto& g : p->wgroups) g.run = tune_run(p->group, g.largest, p->fixed);
     p->chunks = (p->max_entries + p->chunk - 1) / p->chunk;
+    // the persistent launch takes every width group's reduction job at once
+    if (p->persistent && p->wgroups.size() > kMaxRedJobs) return LZK_EUNSUPPORTED;
     // every width group reduces in the same launches, each in its own slice
     // of the reduction scratch
     for (auto& g : p->wgroups) {
@@ -298,6 +450,7 @@ static int create_plan(const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_des
     size_t o_cnt = cv.take<uint32_t>(B), o_off = cv.take<uint32_t>(B + 1);
     size_t o_bsums = cv.take<uint32_t>((B + 4095) / 4096 + 1);
     size_t o_large = cv.take<uint32_t>(p->chunks / kFixSmall + 2);
+    size_t o_bar = cv.take<uint32_t>(2);
     size_t o_ent = cv.take<uint32_t>(std::max<uint64_t>(p->max_entries, 1));
     size_t o_bases = cv.take<Aff<F>>(p->fixed ? 1 : std::max<uint64_t>(p->total_pts, 1));
     size_t o_bsum = cv.take<X>(B);
@@ -314,6 +467,7 @@ static int create_plan(const lzk_msm_desc* msms, size_t n_msm, const lzk_ntt_des
     p->off = reinterpret_cast<uint32_t*>(b + o_off);
     p->bsums = reinterpret_cast<uint32_t*>(b + o_bsums);
     p->large = reinterpret_cast<uint32_t*>(b + o_large);
+    p->bar = reinterpret_cast<uint32_t*>(b + o_bar);
     p->ent = reinterpret_cast<uint32_t*>(b + o_ent);
     p->bases = b + o_bases;
     p->bsum = b + o_bsum;
@@ -377,13 +531,14 @@ int lzk_batch_plan_create_ex(int group, const lzk_msm_desc* msms, size_t n_msm, 
                              size_t n_ntt, uint32_t flags, lzk_batch_plan** out)
 {
     if (!out || (group != 1 && group != 2) || (n_msm && !msms) || (n_ntt && !ntts)) return LZK_EINVAL;
-    if (flags & ~LZK_BATCH_FIXED_BASES) return LZK_EINVAL;
+    if (flags & ~(LZK_BATCH_FIXED_BASES | LZK_BATCH_PERSISTENT)) return LZK_EINVAL;
     *out = nullptr;
     lzk_batch_plan* p = new (std::nothrow) lzk_batch_plan();
     if (!p) return LZK_ENOMEM;
     p->group = group;
     p->flags = flags;
     p->fixed = (flags & LZK_BATCH_FIXED_BASES) != 0;
+    p->persistent = (flags & LZK_BATCH_PERSISTENT) != 0;
     int rc = group == 2 ? create_plan<Fq2>(msms, n_msm, ntts, n_ntt, p) : create_plan<Fq>(msms, n_msm, ntts, n_ntt, p);
     if (rc != LZK_OK) { destroy_plan(p); return rc; }
     *out = p;
@@ -400,6 +555,15 @@ int lzk_batch_plan_run(lzk_batch_plan* p, int use_graph, void* stream)
 {
     if (!p) return LZK_EINVAL;
     cudaStream_t st = as_stream(stream);
+    if (p->persistent) {
+        // eager, and synchronous: the run ends by reading the persistent
+        // launch's barrier error word
+        LZK_TRY(run_all(p, st));
+        uint32_t err = 0;
+        LZK_CUDA(cudaMemcpyAsync(&err, p->bar + 1, sizeof(err), cudaMemcpyDeviceToHost, st));
+        LZK_CUDA(cudaStreamSynchronize(st));
+        return err ? LZK_ETIMEOUT : LZK_OK;
+    }
     if (!use_graph) return run_all(p, st);
     if (!st) return LZK_EINVAL;   // the legacy stream cannot be captured
     if (!p->exec) {

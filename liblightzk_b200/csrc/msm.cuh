@@ -163,19 +163,16 @@ __device__ __forceinline__ Aff<F> load_base(const void* bases, uint32_t v)
     return p;
 }
 
-// 128-thread blocks; at most 168 registers for G1 (3 blocks = 12 warps per
-// SM) and 255 for G2 (2 blocks).  With the products on the FP64 pipe the
-// tighter register bounds make the product calls spill: G1 at 3 blocks/SM
-// measured 6 % faster than at 5 (which matched 4 and 6), G2 at 2 blocks 10 %
-// faster than at 3 and 16 % faster than at 4.
+// The work of one accumulation thread, chunk t (k_accumulate below; the
+// persistent batch kernel runs it too).
 template <class F, int LAYOUT>
-__global__ void __launch_bounds__(128, sizeof(F) == 32 ? 3 : 2) k_accumulate(const void* __restrict__ bases, const uint32_t* __restrict__ ent,
-                                                    const uint32_t* __restrict__ off, uint32_t B, size_t chunks,
-                                                    uint32_t chunk, uint64_t nbases, XYZZ<F>* __restrict__ bsum,
-                                                    XYZZ<F>* __restrict__ head, XYZZ<F>* __restrict__ tail)
+__device__ __forceinline__ void accumulate_chunk(uint64_t t, const void* __restrict__ bases,
+                                                 const uint32_t* __restrict__ ent, const uint32_t* __restrict__ off,
+                                                 uint32_t B, size_t chunks, uint32_t chunk, uint64_t nbases,
+                                                 XYZZ<F>* __restrict__ bsum, XYZZ<F>* __restrict__ head,
+                                                 XYZZ<F>* __restrict__ tail)
 {
     (void)nbases;   // the base records behind the entries (debug checks)
-    uint64_t t = gtid();
     if (t >= chunks) return;
     uint32_t T = off[B];
     uint64_t cs64 = t * chunk;
@@ -212,9 +209,22 @@ __global__ void __launch_bounds__(128, sizeof(F) == 32 ? 3 : 2) k_accumulate(con
     else if (cont_after) st_elem(tail + t, acc);
     else st_elem(bsum + b, acc);
 }
+// 128-thread blocks; at most 168 registers for G1 (3 blocks = 12 warps per
+// SM) and 255 for G2 (2 blocks).  With the products on the FP64 pipe the
+// tighter register bounds make the product calls spill: G1 at 3 blocks/SM
+// measured 6 % faster than at 5 (which matched 4 and 6), G2 at 2 blocks 10 %
+// faster than at 3 and 16 % faster than at 4.
+template <class F, int LAYOUT>
+__global__ void __launch_bounds__(128, sizeof(F) == 32 ? 3 : 2) k_accumulate(const void* __restrict__ bases, const uint32_t* __restrict__ ent,
+                                                    const uint32_t* __restrict__ off, uint32_t B, size_t chunks,
+                                                    uint32_t chunk, uint64_t nbases, XYZZ<F>* __restrict__ bsum,
+                                                    XYZZ<F>* __restrict__ head, XYZZ<F>* __restrict__ tail)
+{
+    accumulate_chunk<F, LAYOUT>(gtid(), bases, ent, off, B, chunks, chunk, nbases, bsum, head, tail);
+}
 
 template <class F>
-__global__ void k_fixup(const uint32_t* __restrict__ off, uint32_t B, uint32_t chunk, uint64_t chunks,
+__device__ __forceinline__ void fixup_items(const uint32_t* __restrict__ off, uint32_t B, uint32_t chunk, uint64_t chunks,
                         XYZZ<F>* __restrict__ bsum, const XYZZ<F>* __restrict__ head, const XYZZ<F>* __restrict__ tail,
                         uint32_t* __restrict__ large)
 {
@@ -234,16 +244,24 @@ __global__ void k_fixup(const uint32_t* __restrict__ off, uint32_t B, uint32_t c
         st_elem(bsum + b, acc);
     }
 }
+template <class F>
+__global__ void k_fixup(const uint32_t* __restrict__ off, uint32_t B, uint32_t chunk, uint64_t chunks,
+                        XYZZ<F>* __restrict__ bsum, const XYZZ<F>* __restrict__ head, const XYZZ<F>* __restrict__ tail,
+                        uint32_t* __restrict__ large)
+{
+    fixup_items<F>(off, B, chunk, chunks, bsum, head, tail, large);
+}
 
 // One block per listed bucket: strided partial sums, then a tree in shared
 // memory.  Partial q of bucket b is tail[c0] (q = 0) or head[c0 + q].
+// (blockDim.x points of shared memory at sm; the persistent batch kernel
+// runs it too)
 template <class F>
-__global__ void k_fixup_large(const uint32_t* __restrict__ off, uint32_t chunk, XYZZ<F>* __restrict__ bsum,
-                              const XYZZ<F>* __restrict__ head, const XYZZ<F>* __restrict__ tail,
-                              const uint32_t* __restrict__ large)
+__device__ __forceinline__ void fixup_large_items(const uint32_t* __restrict__ off, uint32_t chunk,
+                                                  XYZZ<F>* __restrict__ bsum, const XYZZ<F>* __restrict__ head,
+                                                  const XYZZ<F>* __restrict__ tail, const uint32_t* __restrict__ large,
+                                                  XYZZ<F>* sm)
 {
-    extern __shared__ uint4 fx_raw[];
-    XYZZ<F>* sm = reinterpret_cast<XYZZ<F>*>(fx_raw);
     uint32_t nl = large[0];
     for (uint32_t idx = blockIdx.x; idx < nl; idx += gridDim.x) {
         uint32_t b = large[1 + idx];
@@ -261,6 +279,14 @@ __global__ void k_fixup_large(const uint32_t* __restrict__ off, uint32_t chunk, 
         if (threadIdx.x == 0) st_elem(bsum + b, ld_elem(sm));
         __syncthreads();
     }
+}
+template <class F>
+__global__ void k_fixup_large(const uint32_t* __restrict__ off, uint32_t chunk, XYZZ<F>* __restrict__ bsum,
+                              const XYZZ<F>* __restrict__ head, const XYZZ<F>* __restrict__ tail,
+                              const uint32_t* __restrict__ large)
+{
+    extern __shared__ uint4 fx_raw[];
+    fixup_large_items<F>(off, chunk, bsum, head, tail, large, reinterpret_cast<XYZZ<F>*>(fx_raw));
 }
 
 // Warp shuffles of whole points
@@ -382,7 +408,7 @@ __device__ __forceinline__ uint32_t red_job_of(const RedJobs<F>& jobs, uint64_t 
 }
 
 template <class F>
-__global__ void __launch_bounds__(128) k_red_tile(const __grid_constant__ RedJobs<F> jobs, uint64_t total)
+__device__ __forceinline__ void red_tile_items(const RedJobs<F>& jobs, uint64_t total)
 {
     const uint32_t lane = threadIdx.x & 31;
     for (uint64_t item = gtid() >> 5; item < total; item += gstride() >> 5) {
@@ -414,10 +440,15 @@ __global__ void __launch_bounds__(128) k_red_tile(const __grid_constant__ RedJob
         }
     }
 }
+template <class F>
+__global__ void __launch_bounds__(128) k_red_tile(const __grid_constant__ RedJobs<F> jobs, uint64_t total)
+{
+    red_tile_items<F>(jobs, total);
+}
 
 
 template <class F>
-__global__ void __launch_bounds__(128) k_red_slices(const __grid_constant__ RedJobs<F> jobs, uint64_t total)
+__device__ __forceinline__ void red_slices_items(const RedJobs<F>& jobs, uint64_t total)
 {
     const uint32_t lane = threadIdx.x & 31;
     for (uint64_t item = gtid() >> 5; item < total; item += gstride() >> 5) {
@@ -438,9 +469,14 @@ __global__ void __launch_bounds__(128) k_red_slices(const __grid_constant__ RedJ
         if (lane == 0) st_elem(J.part + g, x);
     }
 }
+template <class F>
+__global__ void __launch_bounds__(128) k_red_slices(const __grid_constant__ RedJobs<F> jobs, uint64_t total)
+{
+    red_slices_items<F>(jobs, total);
+}
 
 template <class F>
-__global__ void __launch_bounds__(128) k_red_scale(const __grid_constant__ RedJobs<F> jobs, uint64_t total)
+__device__ __forceinline__ void red_scale_items(const RedJobs<F>& jobs, uint64_t total)
 {
     const uint32_t lane = threadIdx.x & 31;
     for (uint64_t item = gtid() >> 5; item < total; item += gstride() >> 5) {
@@ -462,9 +498,14 @@ __global__ void __launch_bounds__(128) k_red_scale(const __grid_constant__ RedJo
         if (lane == 0) st_elem(J.scaled + g, x);
     }
 }
+template <class F>
+__global__ void __launch_bounds__(128) k_red_scale(const __grid_constant__ RedJobs<F> jobs, uint64_t total)
+{
+    red_scale_items<F>(jobs, total);
+}
 
 template <class F>
-__global__ void __launch_bounds__(128) k_red_combine(const __grid_constant__ RedJobs<F> jobs, uint64_t total)
+__device__ __forceinline__ void red_combine_items(const RedJobs<F>& jobs, uint64_t total)
 {
     const uint32_t lane = threadIdx.x & 31;
     for (uint64_t item = gtid() >> 5; item < total; item += gstride() >> 5) {
@@ -475,6 +516,11 @@ __global__ void __launch_bounds__(128) k_red_combine(const __grid_constant__ Red
         for (uint32_t d = 16; d > 0; d >>= 1) x = xyzz_add_cold(x, shfl_xor_pt(x, d));
         if (lane == 0) st_elem(J.win + w, x);
     }
+}
+template <class F>
+__global__ void __launch_bounds__(128) k_red_combine(const __grid_constant__ RedJobs<F> jobs, uint64_t total)
+{
+    red_combine_items<F>(jobs, total);
 }
 
 // Scratch points each of R, T, part and scaled needs for wb sets of m

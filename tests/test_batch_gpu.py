@@ -1,7 +1,9 @@
 """Batched MSMs and NTTs of uneven sizes (lzk_batch_plan_*): every result of
 the batch equals the oracle's, eagerly and through the captured CUDA graph
 (first run captures, second replays) after the inputs changed in place, with
-plain bases and with the shifted-copy tables of LZK_BATCH_FIXED_BASES."""
+plain bases and with the shifted-copy tables of LZK_BATCH_FIXED_BASES, and
+with the MSM phases as one persistent launch (LZK_BATCH_PERSISTENT: runs are
+eager whatever use_graph says)."""
 import numpy as np
 import pytest
 
@@ -21,9 +23,10 @@ def _host(t):
     return device.to_host(t)
 
 
+@pytest.mark.parametrize("persistent", [False, True])
 @pytest.mark.parametrize("fixed_bases", [False, True])
 @pytest.mark.parametrize("group", [1, 2])
-def test_batch_plan(cuda, orc, rng_state, group, fixed_bases):
+def test_batch_plan(cuda, orc, rng_state, group, fixed_bases, persistent):
     import torch
 
     from liblightzk_b200 import batch
@@ -40,7 +43,8 @@ def test_batch_plan(cuda, orc, rng_state, group, fixed_bases):
     outs = [torch.empty((3, 4) if group == 1 else (3, 2, 4), dtype=torch.int64, device="cuda") for _ in sizes]
     dev_n = [_dev(np.zeros((1 << k, 4), np.uint64)) for k, _ in nspec]
     plan = batch.BatchPlan(group, [(s, b, o, w) for s, b, o, w in zip(dev_s, dev_b, outs, wins)],
-                           [(d, k, di) for d, (k, di) in zip(dev_n, nspec)], fixed_bases=fixed_bases)
+                           [(d, k, di) for d, (k, di) in zip(dev_n, nspec)], fixed_bases=fixed_bases,
+                           persistent=persistent)
     stream = torch.cuda.Stream()
     for mode in ("eager", "capture", "replay"):
         hs = [scalars(orc, n, rng_state) if n else np.zeros((0, 4), np.uint64) for n in sizes]

@@ -5,7 +5,8 @@ against the oracle.
   2^10..2^20 points drawn log-uniformly, over slices of one pool of 2^20
   random points, and 32 Fr NTTs of 2^12..2^22 elements in all four
   directions), run as one plan through its captured CUDA graph, with plain
-  bases and with shifted-copy tables built at creation; every MSM
+  bases and with shifted-copy tables built at creation, and as the
+  persistent launch over the tables; every MSM
   result equals the oracle's MSM (the reference checks its MSM the same
   way, GPU against CPU, test/msm-check.cu:45-58) and every NTT output the
   oracle's transform, element for element.
@@ -30,7 +31,8 @@ def _host(t):
 
 
 def test_batched_workload_against_oracle(cuda, orc):
-    """both plan forms: plain bases, and shifted-copy tables built at creation"""
+    """the plan forms: plain bases, shifted-copy tables built at creation, and
+    tables with the MSM phases as one persistent launch"""
     import torch
 
     from liblightzk_b200 import batch
@@ -42,8 +44,8 @@ def test_batched_workload_against_oracle(cuda, orc):
     want_msm = [orc.msm(1, _host(s), _host(b)) for s, b, _ in msms]
     want_ntt = [orc.ntt(h, k, di) for (_, k, di), h in zip(ntts, ntt_in)]
     stream = torch.cuda.Stream()
-    for fixed in (False, True):
-        plan = batch.BatchPlan(1, msms, ntts, fixed_bases=fixed)
+    for fixed, persistent in ((False, False), (True, False), (True, True)):
+        plan = batch.BatchPlan(1, msms, ntts, fixed_bases=fixed, persistent=persistent)
         for _ in range(2):        # captures the graph, then replays it on fresh NTT inputs
             for (d, _, _), h in zip(ntts, ntt_in):
                 d.copy_(torch.from_numpy(h.view(np.int64)).to(d.device))
@@ -51,9 +53,9 @@ def test_batched_workload_against_oracle(cuda, orc):
             plan.run(use_graph=True, stream=stream)
             torch.cuda.synchronize()
         for (s, b, o), want in zip(msms, want_msm):
-            assert same_point(orc, 1, _host(o), want), f"MSM of {s.shape[0]} points (fixed bases {fixed})"
+            assert same_point(orc, 1, _host(o), want), f"MSM of {s.shape[0]} points ({fixed=}, {persistent=})"
         for (d, k, di), want in zip(ntts, want_ntt):
-            assert (_host(d) == want).all(), f"NTT 2^{k} direction {di} (fixed bases {fixed})"
+            assert (_host(d) == want).all(), f"NTT 2^{k} direction {di} ({fixed=}, {persistent=})"
         plan.close()
 
 
