@@ -5,26 +5,26 @@
 // mont_t.cuh:396-430, 208-302, 465-629) and of fp2_t (alt_bn128_t.cuh:
 // 97-224), applied to arrays.  Each operation runs through the same device
 // routines the operators use: Fq and Fq2 products and squares through the
-// out-of-line bodies of the curve formulas (mul_call, fq2_mul_call with its
-// lazily reduced Karatsuba product, fq2_sqr_call), Fr products through the
-// inline product of the NTT butterflies, additions and subtractions through
-// the same carry chains.  Results are canonical (< p).
+// out-of-line bodies of the curve formulas (mul52_call, fq2_mul_call with its
+// lazily reduced Karatsuba product, fq2_sqr_call) and the square of their
+// square pairs (sqr52), Fr products through the product of the NTT
+// butterflies (mul52), all of them on the FP64 pipe (field52.cuh), additions
+// and subtractions through the same carry chains.  Results are canonical
+// (< p).
 #include "common.cuh"
 #include "curve.cuh"
 
 namespace lzk {
 
 template <class F>
-__device__ __forceinline__ F fop_mul(const F& a, const F& b) { return mul(a, b); }
+__device__ __forceinline__ F fop_mul(const F& a, const F& b) { return mul52(a, b); }
 template <>
 __device__ __forceinline__ Fq fop_mul<Fq>(const Fq& a, const Fq& b) { return cmul(a, b); }
 template <>
 __device__ __forceinline__ Fq2 fop_mul<Fq2>(const Fq2& a, const Fq2& b) { return cmul(a, b); }
 
 template <class F>
-__device__ __forceinline__ F fop_sqr(const F& a) { return sqr(a); }
-template <>
-__device__ __forceinline__ Fq fop_sqr<Fq>(const Fq& a) { return csqr(a); }
+__device__ __forceinline__ F fop_sqr(const F& a) { return sqr52(a); }
 template <>
 __device__ __forceinline__ Fq2 fop_sqr<Fq2>(const Fq2& a) { return csqr(a); }
 

@@ -3,7 +3,9 @@ arithmetic: the golden arrays of tests/golden/reference_host_arith.npz were
 computed by the reference's libff code (mont_t / fp2_t semantics,
 mont_t.cuh:396-430, alt_bn128_t.cuh:122-151), so every product, sum,
 inverse and conversion of the device routines that the MSM, NTT and point
-formulas use must equal them bit for bit.  Edge operands beyond the golden
+formulas use must equal them bit for bit: products and squares here run
+through the FP64-pipe forms of field52.cuh (Fq and Fq2 through the curve
+formulas' out-of-line bodies, Fr through the NTT butterflies' product).  Edge operands beyond the golden
 set (0, 1, p - 1, sums at 2p - 2, Fq2 operands whose Karatsuba sums and
 cross terms sit at the reduction bounds) are compared with the C oracle,
 which the golden arrays pin."""
