@@ -489,6 +489,7 @@ def run_tune_case(args):
     t1 = autotune.tune_msm(1, log_ns=range(10, 22), spread=2, reps=2)
     t2 = autotune.tune_msm(2, log_ns=range(10, 21), spread=1, reps=2)
     tt = autotune.tune_msm_table(1, log_ns=range(10, 21), reps=2)
+    tt2 = autotune.tune_msm_table(2, log_ns=range(10, 21), spread=(4, 1), reps=2)
     tn = autotune.tune_ntt(range(10, 25), reps=2)
     circ = synth.Circuit(args.log_m, seed=1)
     pk = synth.ProvingKey(circ, seed=7)
@@ -500,6 +501,8 @@ def run_tune_case(args):
                       "msm_g2": {lg: {k: v[k] for k in ("window", "run", "chunk")} for lg, v in t2.items()},
                       "msm_g1_table": {lg: {k: v[k] for k in ("window", "run", "chunk", "ms", "chunk_ms")}
                                        for lg, v in tt.items()},
+                      "msm_g2_table": {lg: {k: v[k] for k in ("window", "run", "chunk", "ms", "chunk_ms")}
+                                       for lg, v in tt2.items()},
                       "ntt_block": {lg: {"best": v[0], "ms": v[1]} for lg, v in tn.items()},
                       "prover_ms_per_proof": {f"chunk {c}, run {r}": ms for (c, r), ms in tp.items()}}), flush=True)
 
