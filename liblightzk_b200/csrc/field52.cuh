@@ -342,6 +342,38 @@ __device__ __forceinline__ Fp<P> mul52(const Fp<P>& a, const Fp<P>& b)
     return final_sub<P>(t);
 }
 
+// a * b / 2^256 mod p (canonical) with b given already as radix-2^52
+// doubles (to_d52<0>, as a twiddle table stores it), for any 8-limb a with
+// 16 a b < 85 p^2 (a below 2p with b < p qualifies): the drop-in product
+// without b's conversion.
+template <class P>
+__device__ __forceinline__ Fp<P> mul52_pre(const Fp<P>& a, const double db[5])
+{
+    double da[5];
+    to_d52<4>(da, a.v);
+    uint64_t r[5];
+    mont52_core<P>(r, da, db);
+    uint32_t t[8];
+    from_limbs52(t, r);
+    return final_sub<P>(t);
+}
+
+// a + p - b for canonical a, b: in (0, 2p), not reduced (a product operand)
+template <class P>
+__device__ __forceinline__ Fp<P> sub_plus_p(const Fp<P>& a, const Fp<P>& b)
+{
+    Fp<P> r;
+    uint64_t c = 0, d = 0;
+    _Pragma("unroll") for (int i = 0; i < 8; i++) {
+        uint64_t x = (uint64_t)a.v[i] + P::p(i) + c;
+        c = x >> 32;
+        uint64_t y = (uint64_t)(uint32_t)x - b.v[i] - d;
+        d = y >> 63;
+        r.v[i] = (uint32_t)y;
+    }
+    return r;
+}
+
 // Square with the drop-in interface: the operand enters as 4a, so
 // (4a)^2 / 2^260 = a^2 / 2^256, from 15 limb products instead of 25.
 template <class P>

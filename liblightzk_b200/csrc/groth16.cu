@@ -448,10 +448,13 @@ int prove_ctx(const lzk_prover* p, ProveCtx* x, const Fr* z, const lzk_fr_t* r, 
         NttTables t; CosetTables ct;
         LZK_TRY(get_tables(p->log_m, t, ct));
         const Fr* minv = t.consts + 2;
-        LZK_TRY(ntt_passes(x->x, p->log_m, 3, p->L, t.tw[1], false, NttEdge{}, NttEdge{}, st));
-        LZK_TRY(ntt_passes(x->x, p->log_m, 3, p->L, t.tw[0], true, NttEdge{ct.lo[0], ct.hi[0], minv, 1}, NttEdge{}, st));
+        LZK_TRY(ntt_passes(x->x, p->log_m, 3, p->L, t.tw[1], false, NttEdge{}, NttEdge{}, st, nullptr,
+                           twd_for(t, 1, p->log_m)));
+        LZK_TRY(ntt_passes(x->x, p->log_m, 3, p->L, t.tw[0], true, NttEdge{ct.lo[0], ct.hi[0], minv, 1}, NttEdge{}, st,
+                           nullptr, twd_for(t, 0, p->log_m)));
         k_abc<<<grid_for(p->L, 256, sm_count() * 8), 256, 0, st>>>(x0, x1, x2, p->L, p->zinv); note_launch();
-        LZK_TRY(ntt_passes(x0, p->log_m, 1, 0, t.tw[1], false, NttEdge{}, NttEdge{ct.lo[1], ct.hi[1], minv, 1}, st));
+        LZK_TRY(ntt_passes(x0, p->log_m, 1, 0, t.tw[1], false, NttEdge{}, NttEdge{ct.lo[1], ct.hi[1], minv, 1}, st,
+                           nullptr, twd_for(t, 1, p->log_m)));
         hs = x0;
     }
     trace_end(tr_h, st);

@@ -77,6 +77,18 @@ __global__ void k_powers(const Fr* __restrict__ basep, Fr* __restrict__ out, siz
     }
 }
 
+// twiddles in radix-2^52 form: twd[kTwdStride e + i] = limb i of tw[e]
+__global__ void k_tw_to_d52(const Fr* __restrict__ tw, double* __restrict__ twd, size_t count)
+{
+    for (uint64_t e = gtid(); e < count; e += gstride()) {
+        double d[5];
+        to_d52<0>(d, ldg_elem(tw + e).v);
+        double* o = twd + e * kTwdStride;
+        _Pragma("unroll") for (int i = 0; i < 5; i++) o[i] = d[i];
+        o[5] = 0.0;
+    }
+}
+
 static std::mutex g_ntt_mu;
 static std::map<std::pair<int, uint32_t>, NttTables> g_ntt_tables;
 static std::map<int, CosetTables> g_coset_tables;
@@ -99,15 +111,22 @@ int get_tables(uint32_t k, NttTables& out, CosetTables& cos)
         size_t half = k ? (size_t(1) << (k - 1)) : 1;
         if (dev_malloc(reinterpret_cast<void**>(&t.consts), 8 * sizeof(Fr)) != LZK_OK ||
             dev_malloc(reinterpret_cast<void**>(&t.tw[0]), half * sizeof(Fr)) != LZK_OK ||
-            dev_malloc(reinterpret_cast<void**>(&t.tw[1]), half * sizeof(Fr)) != LZK_OK) {
+            dev_malloc(reinterpret_cast<void**>(&t.tw[1]), half * sizeof(Fr)) != LZK_OK ||
+            dev_malloc(reinterpret_cast<void**>(&t.twd[0]), half * kTwdStride * sizeof(double)) != LZK_OK ||
+            dev_malloc(reinterpret_cast<void**>(&t.twd[1]), half * kTwdStride * sizeof(double)) != LZK_OK) {
             cudaFree(t.consts);
             cudaFree(t.tw[0]);
             cudaFree(t.tw[1]);
+            cudaFree(t.twd[0]);
+            cudaFree(t.twd[1]);
             rc = LZK_ENOMEM;
         } else {
             k_ntt_consts<<<1, 32, 0, st>>>(k, t.consts); note_launch();
             k_powers<<<grid_for((half + 63) / 64, 128), 128, 0, st>>>(t.consts + 0, t.tw[0], half); note_launch();
             k_powers<<<grid_for((half + 63) / 64, 128), 128, 0, st>>>(t.consts + 1, t.tw[1], half); note_launch();
+            for (int d = 0; d < 2; d++) {
+                k_tw_to_d52<<<grid_for(half, 128), 128, 0, st>>>(t.tw[d], t.twd[d], half); note_launch();
+            }
             rc = cuda_status(cudaStreamSynchronize(st));
             if (rc == LZK_OK) g_ntt_tables[{dev, k}] = t;
         }
@@ -176,10 +195,24 @@ __device__ __forceinline__ Fr edge_apply(const NttEdge& ed, const Fr& sc, Fr x, 
 //     order in, natural out; with u = w^((j mod 2^t) << (k-1-t)) hi,
 //     c[j] = lo + u, c[j + 2^t] = lo - u.
 // Both compute X_k = sum_j a_j w^(jk).
-template <bool DIT>
+// Twiddle e as the second operand of the product: read from the radix-2^52
+// table (TWD) or converted from the 8x32-bit table.
+template <bool TWD>
+__device__ __forceinline__ Fr tw_mul(const Fr& x, const Fr* __restrict__ tw, const double* __restrict__ twd, size_t e)
+{
+    if (TWD) {
+        const double2* q = reinterpret_cast<const double2*>(twd + e * kTwdStride);
+        double2 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+        const double d[5] = {a.x, a.y, b.x, b.y, c.x};
+        return mul52_pre(x, d);
+    }
+    return mul52(x, ldg_elem(tw + e));
+}
+
+template <bool DIT, bool TWD>
 __global__ void __launch_bounds__(kNttThreads) k_ntt_pass(Fr* __restrict__ data, NttPass p, const Fr* __restrict__ tw,
-                                                           NttEdge pre, NttEdge post, size_t bstride,
-                                                           Fr* const* __restrict__ ptrs)
+                                                           const double* __restrict__ twd, NttEdge pre, NttEdge post,
+                                                           size_t bstride, Fr* const* __restrict__ ptrs)
 {
     extern __shared__ uint4 smem_raw[];
     Fr* sm = reinterpret_cast<Fr*>(smem_raw);
@@ -211,12 +244,13 @@ __global__ void __launch_bounds__(kNttThreads) k_ntt_pass(Fr* __restrict__ data,
             size_t jm = (((size_t)(g & ((1u << hb) - 1))) << p.lowbits) | low;
             Fr lo = ld_elem(sm + i0), hi = ld_elem(sm + i1);
             if (DIT) {
-                Fr u = mul52(hi, ldg_elem(tw + (jm << (p.k - 1 - (p.lowbits + t)))));
+                Fr u = tw_mul<TWD>(hi, tw, twd, jm << (p.k - 1 - (p.lowbits + t)));
                 st_elem(sm + i0, add(lo, u));
                 st_elem(sm + i1, sub(lo, u));
             } else {
                 st_elem(sm + i0, add(lo, hi));
-                st_elem(sm + i1, mul52(sub(lo, hi), ldg_elem(tw + (jm << (p.s0 + t)))));
+                // lo + p - hi, unreduced: the product takes it below 2p
+                st_elem(sm + i1, tw_mul<TWD>(sub_plus_p(lo, hi), tw, twd, jm << (p.s0 + t)));
             }
         }
         __syncthreads();
@@ -261,15 +295,17 @@ int ntt_prepare_launch()
     std::lock_guard<std::mutex> g(mu);
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
         // the largest block the tuning table allows (kMaxNttBlock elements)
-        LZK_CUDA(cudaFuncSetAttribute(k_ntt_pass<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxNttBlock * sizeof(Fr)));
-        LZK_CUDA(cudaFuncSetAttribute(k_ntt_pass<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxNttBlock * sizeof(Fr)));
+        LZK_CUDA(cudaFuncSetAttribute(k_ntt_pass<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxNttBlock * sizeof(Fr)));
+        LZK_CUDA(cudaFuncSetAttribute(k_ntt_pass<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxNttBlock * sizeof(Fr)));
+        LZK_CUDA(cudaFuncSetAttribute(k_ntt_pass<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxNttBlock * sizeof(Fr)));
+        LZK_CUDA(cudaFuncSetAttribute(k_ntt_pass<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxNttBlock * sizeof(Fr)));
         attr_set[dev] = true;
     }
     return LZK_OK;
 }
 
 int ntt_passes(Fr* data, uint32_t k, uint32_t count, size_t bstride, const Fr* tw, bool dit, NttEdge pre,
-               NttEdge post, cudaStream_t st, Fr* const* ptrs)
+               NttEdge post, cudaStream_t st, Fr* const* ptrs, const double* twd)
 {
     if (k == 0 || k > 30 || count == 0 || count > 65535 || (!data && !ptrs) || !tw) return LZK_EINVAL;
     LZK_TRY(ntt_prepare_launch());
@@ -295,10 +331,15 @@ int ntt_passes(Fr* data, uint32_t k, uint32_t count, size_t bstride, const Fr* t
         size_t blocks = (n >> m) / R;
         size_t smem = (size_t)G * R * sizeof(Fr);
         NttEdge a = q == 0 ? pre : NttEdge{}, b = q == P - 1 ? post : NttEdge{};
-        if (dit)
-            k_ntt_pass<true><<<dim3((unsigned)blocks, count), kNttThreads, smem, st>>>(data, pp, tw, a, b, bstride, ptrs);
+        const dim3 grid((unsigned)blocks, count);
+        if (dit && twd)
+            k_ntt_pass<true, true><<<grid, kNttThreads, smem, st>>>(data, pp, tw, twd, a, b, bstride, ptrs);
+        else if (dit)
+            k_ntt_pass<true, false><<<grid, kNttThreads, smem, st>>>(data, pp, tw, twd, a, b, bstride, ptrs);
+        else if (twd)
+            k_ntt_pass<false, true><<<grid, kNttThreads, smem, st>>>(data, pp, tw, twd, a, b, bstride, ptrs);
         else
-            k_ntt_pass<false><<<dim3((unsigned)blocks, count), kNttThreads, smem, st>>>(data, pp, tw, a, b, bstride, ptrs);
+            k_ntt_pass<false, false><<<grid, kNttThreads, smem, st>>>(data, pp, tw, twd, a, b, bstride, ptrs);
         note_launch();
         done += m;
     }
@@ -310,12 +351,12 @@ int ntt_passes(Fr* data, uint32_t k, uint32_t count, size_t bstride, const Fr* t
 // reversal with the output factors.
 static int ntt_enqueue(Fr* data, uint32_t k, uint32_t count, size_t bstride, const Fr* tw, const Fr* scale,
                        const Fr* pre_lo, const Fr* pre_hi, const Fr* post_lo, const Fr* post_hi, cudaStream_t st,
-                       Fr* const* ptrs = nullptr)
+                       Fr* const* ptrs = nullptr, const double* twd = nullptr)
 {
     LZK_TRY(ntt_prepare_launch());
     if (k > 0) {
         NttEdge pre{pre_lo, pre_hi, nullptr, 0};
-        LZK_TRY(ntt_passes(data, k, count, bstride, tw, false, pre, NttEdge{}, st, ptrs));
+        LZK_TRY(ntt_passes(data, k, count, bstride, tw, false, pre, NttEdge{}, st, ptrs, twd));
     } else if (!(scale || post_lo || pre_lo)) {
         return LZK_OK;
     }
@@ -335,7 +376,8 @@ int ntt_run(Fr* data, uint32_t k, int dir, uint32_t count, size_t bstride, const
     const Fr* scale = scale_override ? scale_override : (inv ? t.consts + 2 : nullptr);
     return ntt_enqueue(data, k, count, bstride, t.tw[inv ? 1 : 0], scale,
                        (coset && !inv) ? c.lo[0] : nullptr, (coset && !inv) ? c.hi[0] : nullptr,
-                       (coset && inv) ? c.lo[1] : nullptr, (coset && inv) ? c.hi[1] : nullptr, st, ptrs);
+                       (coset && inv) ? c.lo[1] : nullptr, (coset && inv) ? c.hi[1] : nullptr, st, ptrs,
+                       twd_for(t, inv ? 1 : 0, k));
 }
 
 }  // namespace lzk

@@ -7,8 +7,17 @@ namespace lzk {
 
 struct NttTables {
     Fr* tw[2] = {nullptr, nullptr};  // w^e, w^-e for e < n/2
+    // the same twiddles as radix-2^52 limbs in doubles (the FP64 product's
+    // operand form, field52.cuh), kTwdStride doubles per twiddle
+    double* twd[2] = {nullptr, nullptr};
     Fr* consts = nullptr;            // see k_ntt_consts
 };
+constexpr uint32_t kTwdStride = 6;   // 5 limbs and a pad: 48-byte records, three 16-byte loads
+// Transforms up to 2^kTwdMaxLog read the radix-2^52 table (its 2^(k-1)
+// records of 48 bytes stay in L2); larger ones the 32-byte table, which
+// measured faster there (coset NTT 2^24: 5.91 against 6.01 ms).
+constexpr uint32_t kTwdMaxLog = 21;
+inline const double* twd_for(const NttTables& t, int inv, uint32_t k) { return k <= kTwdMaxLog ? t.twd[inv] : nullptr; }
 
 struct CosetTables {
     Fr* lo[2] = {nullptr, nullptr};  // g^j, g^-j for j < 4096
@@ -41,8 +50,10 @@ int ntt_run(Fr* data, uint32_t k, int dir, uint32_t count, size_t bstride, const
 // The passes of `count` transforms of size 2^k (k >= 1) with twiddle table
 // tw (w^e, e < n/2) and no bit reversal: DIF takes natural order to
 // bit-reversed order, DIT bit-reversed order to natural order.  pre applies
-// to the first pass's loads, post to the last pass's stores.
+// to the first pass's loads, post to the last pass's stores.  twd, when
+// given, is the same table in radix-2^52 form (NttTables::twd), which the
+// butterflies then read instead of converting tw.
 int ntt_passes(Fr* data, uint32_t k, uint32_t count, size_t bstride, const Fr* tw, bool dit, NttEdge pre,
-               NttEdge post, cudaStream_t st, Fr* const* ptrs = nullptr);
+               NttEdge post, cudaStream_t st, Fr* const* ptrs = nullptr, const double* twd = nullptr);
 
 }  // namespace lzk
