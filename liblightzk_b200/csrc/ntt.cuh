@@ -14,8 +14,8 @@ struct NttTables {
 };
 constexpr uint32_t kTwdStride = 6;   // 5 limbs and a pad: 48-byte records, three 16-byte loads
 // Transforms up to 2^kTwdMaxLog read the radix-2^52 table (its 2^(k-1)
-// records of 48 bytes stay in L2); larger ones the 32-byte table, which
-// measured faster there (coset NTT 2^24: 5.91 against 6.01 ms).
+// records of 48 bytes stay in L2); larger ones the 32-byte table (at 2^24
+// both measured the same).
 constexpr uint32_t kTwdMaxLog = 21;
 inline const double* twd_for(const NttTables& t, int inv, uint32_t k) { return k <= kTwdMaxLog ? t.twd[inv] : nullptr; }
 
