@@ -529,6 +529,12 @@ int lzk_trace_timeline(lzk_trace_span* spans, size_t cap, size_t* count);
  * from the call that needed it, with everything it had allocated released);
  * a negative value turns the failures off.  Process-wide. */
 int lzk_debug_fail_allocations(long long after);
+/* Test hook of the persistent batch launch (LZK_BATCH_PERSISTENT): every
+ * grid barrier also waits for extra_arrivals arrivals that never come (0 =
+ * normal) and gives up after max_polls polls (0 = the default, about 2 s),
+ * so a test can make the bounded waits run out and see LZK_ETIMEOUT without
+ * any fault.  No counterpart in the reference. */
+int lzk_debug_persistent_barrier(uint32_t extra_arrivals, uint32_t max_polls);
 /* Debug builds (liblzk_b200_debug.so, compiled with LZK_DEBUG_CHECKS): the
  * digit sort, bucket accumulation and fix-up kernels check every index their
  * inputs imply and, instead of an out-of-range read or write, set a bit of a

@@ -79,6 +79,7 @@ SIGNATURES = {
     "lzk_probe_mont_rate_int": (c_i, [ctypes.POINTER(ctypes.c_double)]),
     "lzk_launch_count": (ctypes.c_uint64, []),
     "lzk_debug_fail_allocations": (c_i, [ctypes.c_longlong]),
+    "lzk_debug_persistent_barrier": (c_i, [ctypes.c_uint32, ctypes.c_uint32]),
     "lzk_debug_check_word": (c_u32, [c_i]),
     "lzk_debug_checks_enabled": (c_i, []),
 }

@@ -18,6 +18,7 @@
 #include "msm.cuh"
 #include "ntt.cuh"
 #include <algorithm>
+#include <atomic>
 #include <map>
 #include <vector>
 
@@ -166,22 +167,25 @@ __global__ void k_bfinish(const BDesc* __restrict__ d, uint32_t count, const XYZ
 // block then leaves at its next barrier, so the kernel always ends; the
 // host reads bar[1] after the run (LZK_ETIMEOUT).
 constexpr uint32_t kBarPolls = 1u << 23;
+// lzk_debug_persistent_barrier: extra arrivals every barrier waits for (so
+// that, when nonzero, none is ever reached) and the poll limit
+static std::atomic<uint32_t> g_persist_extra{0}, g_persist_polls{kBarPolls};
 
-__device__ __forceinline__ bool persist_barrier(uint32_t* bar, uint32_t phase)
+__device__ __forceinline__ bool persist_barrier(uint32_t* bar, uint32_t phase, uint32_t extra, uint32_t max_polls)
 {
     __shared__ uint32_t ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
         atomicAdd(bar, 1u);
-        const uint32_t target = phase * gridDim.x;
+        const uint32_t target = phase * gridDim.x + extra;
         uint32_t good = 1;
         for (uint32_t polls = 0;; polls++) {
             uint32_t v;
             asm volatile("ld.acquire.gpu.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
             if (v >= target) break;
             if (*(volatile uint32_t*)(bar + 1)) { good = 0; break; }
-            if (polls >= kBarPolls) { atomicOr(bar + 1, 1u); good = 0; break; }
+            if (polls >= max_polls) { atomicOr(bar + 1, 1u); good = 0; break; }
             __nanosleep(256);
         }
         __threadfence();
@@ -205,6 +209,7 @@ struct PersistArgs {
     const BDesc* desc;
     uint32_t count;                    // MSMs
     const XYZZ<F>* wres;
+    uint32_t extra, polls;             // barrier arrivals beyond the grid (0; tests only) and poll limit
 };
 
 template <class F>
@@ -215,19 +220,19 @@ k_bpersist(const __grid_constant__ PersistArgs<F> a, const __grid_constant__ Red
     for (uint64_t t = gtid(); t < a.chunks; t += gstride())
         accumulate_chunk<F, LZK_BASES_AFFINE>(t, a.bases, a.ent, a.off, a.B, a.chunks, a.chunk, a.nbases, a.bsum,
                                              a.head, a.tail);
-    if (!persist_barrier(a.bar, 1)) return;
+    if (!persist_barrier(a.bar, 1, a.extra, a.polls)) return;
     fixup_items<F>(a.off, a.B, a.chunk, a.chunks, a.bsum, a.head, a.tail, a.large);
-    if (!persist_barrier(a.bar, 2)) return;
+    if (!persist_barrier(a.bar, 2, a.extra, a.polls)) return;
     fixup_large_items<F>(a.off, a.chunk, a.bsum, a.head, a.tail, a.large, reinterpret_cast<XYZZ<F>*>(fx_raw));
-    if (!persist_barrier(a.bar, 3)) return;
+    if (!persist_barrier(a.bar, 3, a.extra, a.polls)) return;
     red_tile_items<F>(jobs, a.tiles);
-    if (!persist_barrier(a.bar, 4)) return;
+    if (!persist_barrier(a.bar, 4, a.extra, a.polls)) return;
     red_slices_items<F>(jobs, a.nps);
-    if (!persist_barrier(a.bar, 5)) return;
+    if (!persist_barrier(a.bar, 5, a.extra, a.polls)) return;
     red_scale_items<F>(jobs, a.nss);
-    if (!persist_barrier(a.bar, 6)) return;
+    if (!persist_barrier(a.bar, 6, a.extra, a.polls)) return;
     red_combine_items<F>(jobs, a.sets);
-    if (!persist_barrier(a.bar, 7)) return;
+    if (!persist_barrier(a.bar, 7, a.extra, a.polls)) return;
     for (uint64_t k = gtid() >> 5; k < a.count; k += gstride() >> 5) bfinish_one<F>(a.desc, (uint32_t)k, a.wres);
 }
 
@@ -277,6 +282,8 @@ static int run_persistent(lzk_batch_plan* p, cudaStream_t st)
     a.bar = p->bar;
     a.desc = p->d_desc;
     a.count = (uint32_t)p->msm.size();
+    a.extra = g_persist_extra.load();
+    a.polls = g_persist_polls.load();
     a.wres = static_cast<const X*>(p->wres);
     RedJobs<F> jobs = plan_jobs<F>(p, a.tiles, a.nps, a.nss, a.sets);
     int per_sm = 0;
@@ -580,6 +587,13 @@ int lzk_batch_plan_run(lzk_batch_plan* p, int use_graph, void* stream)
         LZK_CUDA(cudaGraphInstantiate(&p->exec, g, 0));
     }
     LZK_CUDA(cudaGraphLaunch(p->exec, st));
+    return LZK_OK;
+}
+
+int lzk_debug_persistent_barrier(uint32_t extra_arrivals, uint32_t max_polls)
+{
+    g_persist_extra.store(extra_arrivals);
+    g_persist_polls.store(max_polls ? max_polls : kBarPolls);
     return LZK_OK;
 }
 

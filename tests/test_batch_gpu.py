@@ -75,3 +75,33 @@ def test_autotuner_installs_measured_widths(cuda):
     for lg, (best, res) in table.items():
         assert best in res and msm.autotune_window(1, 1 << lg) == best
         _capi.call("lzk_msm_set_window", 1, lg, 0)
+
+
+def test_persistent_barrier_timeout_is_reported(cuda, orc, rng_state):
+    """The persistent launch's grid barriers wait with a bound.  With one
+    arrival that never comes and a short poll limit (the test hook
+    lzk_debug_persistent_barrier), every block gives up at the first barrier
+    and leaves, and the run returns LZK_ETIMEOUT (-3) without any fault; the
+    next run with normal barriers gives the oracle's result."""
+    import torch
+
+    from liblightzk_b200 import LzkError, _capi, batch
+    n = 3000
+    hb = bases(orc, 1, n, rng_state)
+    hs = scalars(orc, n, rng_state)
+    s, b = _dev(hs), _dev(hb)
+    out = torch.empty((3, 4), dtype=torch.int64, device="cuda")
+    plan = batch.BatchPlan(1, [(s, b, out)], [], persistent=True)
+    stream = torch.cuda.Stream()
+    _capi.call("lzk_debug_persistent_barrier", 1, 4096)
+    try:
+        with pytest.raises(LzkError) as e:
+            plan.run(stream=stream)
+        assert e.value.status == -3
+    finally:
+        _capi.call("lzk_debug_persistent_barrier", 0, 0)
+    plan.run(stream=stream)
+    torch.cuda.synchronize()
+    want = orc.jac_to_aff(1, orc.msm(1, hs, hb)[None])
+    assert (orc.jac_to_aff(1, _host(out)[None]) == want).all()
+    plan.close()
